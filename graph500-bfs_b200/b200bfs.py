@@ -1,0 +1,318 @@
+"""Host-side binding of the B200 BFS engine (libb200bfs.so, include/b200bfs.h).
+
+`BfsOnB200` mirrors the member surface of the reference's `class BfsBase`
+(mpi/bfs.hpp:48-172), which the benchmark driver reaches as `BfsOnCPU`
+(mpi/bfs_cpu.hpp:13): construct / prepare_bfs / run_bfs / get_pred / end_bfs /
+has_edge, plus a `graph_` facade with pred_size(), has_edge(v) and
+log_orig_global_verts_.  Errors become `B200BfsError` (the reference throws
+`const char*` / std::runtime_error).
+
+There is no CPU fallback: importing this module on a machine without the
+built library or without a CUDA device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libb200bfs.so")
+
+OK = 0
+ERR_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "STATE", 5: "TIMEOUT", 6: "OVERFLOW",
+             7: "NOT_FOUND"}
+
+BUILD_COREBFS = 1 << 0
+BUILD_GROUP_REORDER = 1 << 1
+BUILD_INPUT_SYMMETRIC = 1 << 2
+
+USERSEED1, USERSEED2 = 2, 3  # mpi/parameters.h:204-205
+DEFAULT_ALPHA, DEFAULT_BETA = 10.0, 14.0  # mpi/parameters.h:97-98
+AUTO_NUM = 9
+AUTO_NOT_DEFINED = -1
+
+# Exported symbols (must match include/b200bfs.h).
+SYMBOLS = [
+    "b200bfs_create", "b200bfs_destroy", "b200bfs_last_error", "b200bfs_print_information",
+    "b200bfs_build_from_edges", "b200bfs_build_from_packed", "b200bfs_generate_graph",
+    "b200bfs_generate_edges", "b200bfs_graph_info_get", "b200bfs_get_csr", "b200bfs_has_edge",
+    "b200bfs_has_edge_all", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
+    "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
+    "b200bfs_validate",
+]
+
+
+class B200BfsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"b200bfs error {code} ({ERR_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_uint64)]
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [("scale", ctypes.c_int32), ("reorder_bits", ctypes.c_int32),
+                ("pred_size", ctypes.c_int64), ("num_global_edges", ctypes.c_int64),
+                ("num_global_verts", ctypes.c_int64), ("num_rows", ctypes.c_int64),
+                ("num_input_edges", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("corebfs", ctypes.c_int32), ("prune_rounds", ctypes.c_int32),
+                ("core_vertices", ctypes.c_int64), ("tree_vertices", ctypes.c_int64)]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int32), ("num_td_levels", ctypes.c_int32),
+                ("num_bu_levels", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
+                ("bu_level_mask", ctypes.c_uint64), ("visited", ctypes.c_int64),
+                ("edges_scanned_td", ctypes.c_int64), ("edges_scanned_bu", ctypes.c_int64),
+                ("algorithmic_bytes", ctypes.c_int64), ("td_bytes", ctypes.c_int64),
+                ("bu_bytes", ctypes.c_int64), ("device_ms", ctypes.c_double),
+                ("td_ms", ctypes.c_double), ("bu_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libb200bfs.so and declares the C ABI; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise B200BfsError(2, f"{path} is not built; run __graft_entry__.build()")
+    L = ctypes.CDLL(path)
+    P, i64, i32, u64, dbl, vp = (ctypes.POINTER, ctypes.c_int64, ctypes.c_int, ctypes.c_uint64,
+                                 ctypes.c_double, ctypes.c_void_p)
+    H = ctypes.c_void_p
+    L.b200bfs_create.argtypes = [P(Config), P(H)]
+    L.b200bfs_destroy.argtypes = [H]
+    L.b200bfs_last_error.argtypes = [H]
+    L.b200bfs_last_error.restype = ctypes.c_char_p
+    L.b200bfs_print_information.argtypes = [H, ctypes.c_char_p, ctypes.c_size_t]
+    L.b200bfs_build_from_edges.argtypes = [H, vp, i64, i32, i32]
+    L.b200bfs_build_from_packed.argtypes = [H, vp, i64, i32, i32]
+    L.b200bfs_generate_graph.argtypes = [H, i32, i32, u64, u64, i32]
+    L.b200bfs_generate_edges.argtypes = [H, i32, u64, u64, i64, i64, vp]
+    L.b200bfs_graph_info_get.argtypes = [H, P(GraphInfo)]
+    L.b200bfs_get_csr.argtypes = [H, vp, vp, vp, vp]
+    L.b200bfs_has_edge.argtypes = [H, i64, P(ctypes.c_int)]
+    L.b200bfs_has_edge_all.argtypes = [H, vp]
+    L.b200bfs_prepare.argtypes = [H, i32, dbl, dbl]
+    L.b200bfs_run.argtypes = [H, i64, i32, dbl, dbl, vp]
+    L.b200bfs_get_pred.argtypes = [H, vp]
+    L.b200bfs_get_levels.argtypes = [H, vp]
+    L.b200bfs_get_run_stats.argtypes = [H, P(RunStats)]
+    L.b200bfs_get_stream.argtypes = [H, P(ctypes.c_void_p)]
+    L.b200bfs_end.argtypes = [H]
+    L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Engine:
+    """Thin owner of one b200bfs handle."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0):
+        self.L = load_library()
+        cfg = Config(device, 0, hbm_budget_bytes)
+        h = ctypes.c_void_p()
+        rc = self.L.b200bfs_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != OK:
+            raise B200BfsError(rc, "b200bfs_create failed (no CUDA device?)")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.b200bfs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != OK:
+            raise B200BfsError(rc, self.L.b200bfs_last_error(self.h).decode())
+
+    def info(self):
+        gi = GraphInfo()
+        self.check(self.L.b200bfs_graph_info_get(self.h, ctypes.byref(gi)))
+        return gi
+
+    def print_information(self):
+        buf = ctypes.create_string_buffer(512)
+        self.check(self.L.b200bfs_print_information(self.h, buf, 512))
+        return buf.value.decode()
+
+    def generate_graph(self, scale, edgefactor=16, seed1=USERSEED1, seed2=USERSEED2, flags=0):
+        self.check(self.L.b200bfs_generate_graph(self.h, scale, edgefactor, seed1, seed2, flags))
+
+    def generate_edges(self, scale, start, end, seed1=USERSEED1, seed2=USERSEED2):
+        out = np.empty((end - start, 2), dtype=np.int64)
+        self.check(self.L.b200bfs_generate_edges(self.h, scale, seed1, seed2, start, end,
+                                                 _ptr(out)))
+        return out
+
+    def build_from_edges(self, edges, scale=0, flags=0):
+        edges = np.ascontiguousarray(edges, dtype=np.int64)
+        self.check(self.L.b200bfs_build_from_edges(self.h, _ptr(edges), edges.shape[0], scale,
+                                                   flags))
+
+    def build_from_packed(self, packed, scale=0, flags=0):
+        packed = np.ascontiguousarray(packed, dtype=np.uint32)
+        self.check(self.L.b200bfs_build_from_packed(self.h, _ptr(packed), packed.shape[0],
+                                                    scale, flags))
+
+    def get_csr(self):
+        """(row_ptr, col, inv, mdeg) of the searched CSR, in host memory."""
+        gi = self.info()
+        R, E = gi.num_rows, gi.num_global_edges
+        row_ptr = np.empty(R + 1, np.int64)
+        col = np.empty(E, np.int32)
+        inv = np.empty(R, np.int32)
+        mdeg = np.empty(R, np.int32)
+        self.check(self.L.b200bfs_get_csr(self.h, _ptr(row_ptr), _ptr(col), _ptr(inv),
+                                          _ptr(mdeg)))
+        return row_ptr, col, inv, mdeg
+
+    def has_edge(self, v):
+        out = ctypes.c_int()
+        self.check(self.L.b200bfs_has_edge(self.h, v, ctypes.byref(out)))
+        return bool(out.value)
+
+    def has_edge_all(self):
+        out = np.empty(self.info().pred_size, dtype=np.uint8)
+        self.check(self.L.b200bfs_has_edge_all(self.h, _ptr(out)))
+        return out
+
+    def prepare(self, edgefactor=16, alpha=DEFAULT_ALPHA, beta=DEFAULT_BETA):
+        self.check(self.L.b200bfs_prepare(self.h, edgefactor, alpha, beta))
+
+    def run(self, root, edgefactor=16, alpha=DEFAULT_ALPHA, beta=DEFAULT_BETA, at=None):
+        if at is None:
+            at = np.full(AUTO_NUM, AUTO_NOT_DEFINED, dtype=np.int64)
+        self.check(self.L.b200bfs_run(self.h, int(root), edgefactor, alpha, beta, _ptr(at)))
+        return at
+
+    def get_pred(self, out=None):
+        if out is None:
+            out = np.empty(self.info().pred_size, dtype=np.int64)
+        self.check(self.L.b200bfs_get_pred(self.h, _ptr(out)))
+        return out
+
+    def get_levels(self):
+        out = np.empty(self.info().pred_size, dtype=np.int32)
+        self.check(self.L.b200bfs_get_levels(self.h, _ptr(out)))
+        return out
+
+    def run_stats(self):
+        rs = RunStats()
+        self.check(self.L.b200bfs_get_run_stats(self.h, ctypes.byref(rs)))
+        return rs
+
+    def stream(self):
+        """The engine's cudaStream_t as an integer handle."""
+        out = ctypes.c_void_p()
+        self.check(self.L.b200bfs_get_stream(self.h, ctypes.byref(out)))
+        return out.value or 0
+
+    def end(self):
+        self.check(self.L.b200bfs_end(self.h))
+
+    def validate(self, root):
+        err = ctypes.c_int64()
+        cnt = ctypes.c_int64()
+        self.check(self.L.b200bfs_validate(self.h, int(root), ctypes.byref(err),
+                                           ctypes.byref(cnt)))
+        return err.value, cnt.value
+
+
+class _GraphFacade:
+    """The part of Graph2DCSR the driver reads (graph_constructor.hpp:187-333)."""
+
+    def __init__(self, bfs):
+        self._bfs = bfs
+
+    @property
+    def log_orig_global_verts_(self):
+        return self._bfs.engine.info().scale
+
+    @property
+    def reorder_bits_(self):
+        return self._bfs.engine.info().reorder_bits
+
+    @property
+    def num_global_edges_(self):
+        return self._bfs.engine.info().num_global_edges
+
+    @property
+    def num_global_verts_(self):
+        return self._bfs.engine.info().num_global_verts
+
+    def pred_size(self):
+        return self._bfs.engine.info().pred_size
+
+    def has_edge(self, v):
+        return self._bfs.engine.has_edge(v)
+
+
+class BfsOnB200:
+    """Drop-in for BfsBase / BfsOnCPU (mpi/bfs.hpp:48-172, mpi/bfs_cpu.hpp:13)."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0):
+        self.engine = Engine(device, hbm_budget_bytes)
+        self.graph_ = _GraphFacade(self)
+        self._corebfs = False
+
+    @staticmethod
+    def printInformation(validation_level=2, pre_exec=False, real_benchmark=False):
+        return Engine().print_information()
+
+    def construct(self, scale, corebfs_enabled, sym_edge_list):
+        """BfsBase::construct (bfs.hpp:116-139): sym_edge_list is the
+        symmetric (v0, v1) list produced by make_symmetry_edge_list."""
+        flags = BUILD_INPUT_SYMMETRIC | (BUILD_COREBFS if corebfs_enabled else 0)
+        self._corebfs = corebfs_enabled
+        self.engine.build_from_edges(sym_edge_list, scale, flags)
+
+    def construct_generated(self, scale, edgefactor=16, corebfs_enabled=False,
+                            group_reorder=False):
+        """generate_graph_spec2010 + make_symmetry_edge_list + construct
+        (main.cc:412-435) entirely on the device."""
+        flags = (BUILD_COREBFS if corebfs_enabled else 0) | (
+            BUILD_GROUP_REORDER if group_reorder else 0)
+        self._corebfs = corebfs_enabled
+        self.engine.generate_graph(scale, edgefactor, flags=flags)
+
+    def prepare_bfs(self, validation_level, pre_exec, real_benchmark, edgefactor, alpha, beta,
+                    pred=None):
+        self.engine.prepare(edgefactor, alpha, beta)
+
+    def run_bfs(self, root, pred, edgefactor, alpha, beta, auto_tuning_data):
+        """BfsBase::run_bfs (bfs.hpp:3214); pred is filled by get_pred."""
+        at = auto_tuning_data
+        if at is None:
+            at = np.full(AUTO_NUM, AUTO_NOT_DEFINED, dtype=np.int64)
+        self.engine.run(root, edgefactor, alpha, beta, at)
+        self._pred_out = pred
+
+    def get_pred(self, pred):
+        """BfsBase::get_pred (bfs.hpp:161-163): device -> host copy of pred."""
+        self.engine.get_pred(pred)
+
+    def end_bfs(self):
+        self.engine.end()
+
+    def has_edge(self, root):
+        return self.engine.has_edge(root)

@@ -1,0 +1,583 @@
+// Direction-optimizing BFS over the device CSR.
+//
+// One search = BfsBase::run_bfs_core (mpi/bfs.hpp:3238-3609) on one GPU:
+//   initialize_memory (:315-349)  -> init_kernel (pred = -1, visited = 0)
+//   first_expand (:562-631)        -> root_kernel (pred[root] = root)
+//   top_down_search (:1355-1418)   -> td_expand_kernel: edge-balanced
+//       expansion of the frontier queue; each warp takes a tile of 256
+//       adjacency entries of the concatenated frontier rows, reads them
+//       coalesced and claims unvisited neighbours with a race-tolerant pred
+//       store plus a non-returning OR into the visited bitmap (any of several
+//       same-level parents is a valid BFS parent, as validate.hpp accepts);
+//   bottom_up_search_bitmap (:2828-2847, block scan :2184-2414)
+//                                  -> bu_kernel: a warp owns 32 vertices (one
+//       bitmap word); each unvisited lane probes its first neighbours (highest
+//       degree first, so hits come early), the warp then sweeps the remaining
+//       long rows cooperatively; the next bitmap word is built with
+//       __ballot_sync and written once, so no atomics are needed;
+//   expand / frontier bookkeeping (:634-1038)
+//                                  -> frontier_count/scan/write kernels that
+//       turn the new bitmap bits into the next queue with its degree prefix;
+//   direction switch (:3413-3457)  -> host, from the per-level counters.
+#include <algorithm>
+#include <cstring>
+#include "common.cuh"
+#include "bfs_internal.h"
+
+namespace b200bfs {
+namespace {
+
+constexpr int kWordsPerBlock = 256;  // frontier kernels: one thread per word
+constexpr int kTdTile = 256;         // adjacency entries per warp tile
+
+__device__ __forceinline__ void warp_inclusive_scan2(int64_t& a, int64_t& b) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t ta = __shfl_up_sync(kFull, a, o);
+    int64_t tb = __shfl_up_sync(kFull, b, o);
+    if (lane >= o) {
+      a += ta;
+      b += tb;
+    }
+  }
+}
+
+__global__ void init_kernel(int64_t* __restrict__ pred, int64_t pred_size,
+                            uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1, int64_t W,
+                            int64_t R) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // pred in 16-byte stores
+  longlong2* p2 = reinterpret_cast<longlong2*>(pred);
+  const int64_t n2 = pred_size >> 1;
+  for (int64_t i = t0; i < n2; i += stride) p2[i] = make_longlong2(-1, -1);
+  if (t0 == 0 && (pred_size & 1)) pred[pred_size - 1] = -1;
+  for (int64_t w = t0; w < W; w += stride) {
+    // bits at or beyond R are padding and start "visited"
+    int64_t first = w * 32;
+    uint32_t v = 0;
+    if (first + 32 > R) v = (first >= R) ? kFull : (kFull << (R - first));
+    vis0[w] = v;
+    vis1[w] = v;
+  }
+}
+
+__global__ void root_kernel(int64_t root, const int32_t* __restrict__ rank,
+                            const int64_t* __restrict__ row_ptr, int64_t* __restrict__ pred,
+                            uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1,
+                            int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
+                            Counters* ctr) {
+  pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
+  int32_t r = rank[root];
+  memset(ctr, 0, sizeof(Counters));
+  if (r >= 0) {
+    vis0[r >> 5] |= 1u << (r & 31);
+    vis1[r >> 5] |= 1u << (r & 31);
+    queue[0] = r;
+    qdeg[0] = 0;
+    qdeg[1] = row_ptr[r + 1] - row_ptr[r];
+    ctr->qsize = 1;
+    ctr->qedges = qdeg[1];
+  } else {
+    ctr->qsize = 0;
+    qdeg[0] = 0;
+  }
+}
+
+// Edge-balanced top-down expansion.  Frontier queue[0..qsize) with
+// qdeg[i] = sum of degrees of queue[0..i) (qdeg[qsize] = total).
+__global__ void __launch_bounds__(256) td_expand_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  const int64_t qsize = (int64_t)ctr->qsize;
+  if (qsize == 0) return;
+  const int64_t total = qdeg[qsize];
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (total + kTdTile - 1) / kTdTile;
+  for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
+    const int64_t t0 = tile * kTdTile;
+    int64_t i0 = 0;
+    if (lane == 0) {
+      int64_t lo = 0, hi = qsize - 1;  // largest i with qdeg[i] <= t0
+      while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (qdeg[mid] <= t0) lo = mid;
+        else hi = mid - 1;
+      }
+      i0 = lo;
+    }
+    int64_t i = __shfl_sync(kFull, i0, 0);
+    int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
+    int32_t src = queue[i];
+    int64_t rbeg = row_ptr[src];
+#pragma unroll 1
+    for (int k = 0; k < kTdTile / 32; ++k) {
+      const int64_t e = t0 + k * 32 + lane;
+      if (e >= total) break;
+      while (e >= seg_hi) {
+        ++i;
+        seg_lo = seg_hi;
+        seg_hi = qdeg[i + 1];
+        src = queue[i];
+        rbeg = row_ptr[src];
+      }
+      const int32_t u = __ldg(col + rbeg + (e - seg_lo));
+      const uint32_t bit = 1u << (u & 31);
+      // plain load: vis is being updated by this kernel; a stale word only
+      // causes a redundant (still valid) claim
+      if ((vis[u >> 5] & bit) == 0) {
+        pred[__ldg(inv + u)] = pred_entry(__ldg(inv + src), level);
+        red_or(vis + (u >> 5), bit);
+      }
+    }
+  }
+}
+
+// Bottom-up step.  cur is the visited bitmap before this level (read-only
+// here); nxt receives cur | newly found bits for every word.
+template <int kProbe>
+__global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cur,
+                                                 uint32_t* __restrict__ nxt, int64_t W,
+                                                 const int64_t* __restrict__ row_ptr,
+                                                 const int32_t* __restrict__ col,
+                                                 const int32_t* __restrict__ inv,
+                                                 int64_t* __restrict__ pred, int64_t level,
+                                                 Counters* __restrict__ ctr) {
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long found_total = 0, scanned = 0;
+  for (int64_t w = gw; w < W; w += nwarps) {
+    const uint32_t c = cur[w];
+    if (c == kFull) {
+      if (lane == 0) nxt[w] = c;
+      continue;
+    }
+    const int64_t v = w * 32 + lane;
+    const bool active = ((~c) >> lane) & 1u;
+    int64_t b = 0, e = 0;
+    int32_t parent = -1;
+    if (active) {
+      b = row_ptr[v];
+      e = row_ptr[v + 1];
+      const int64_t lim = min(e, b + (int64_t)kProbe);
+      for (; b < lim; ++b) {
+        const int32_t u = __ldg(col + b);
+        ++scanned;
+        if (bit_test(cur, u)) {
+          parent = u;
+          break;
+        }
+      }
+    }
+    unsigned rem = __ballot_sync(kFull, active && parent < 0 && b < e);
+    while (rem) {
+      const int l = __ffs(rem) - 1;
+      rem &= rem - 1;
+      const int64_t jb = __shfl_sync(kFull, b, l), je = __shfl_sync(kFull, e, l);
+      int32_t p = -1;
+      int64_t j = jb;
+      for (; j < je; j += 32) {
+        const int64_t jj = j + lane;
+        int32_t u = 0;
+        bool hit = false;
+        if (jj < je) {
+          u = __ldg(col + jj);
+          hit = bit_test(cur, u);
+        }
+        const unsigned hm = __ballot_sync(kFull, hit);
+        if (hm) {
+          const int fl = __ffs(hm) - 1;
+          p = __shfl_sync(kFull, u, fl);
+          if (lane == l) scanned += (unsigned long long)(j - jb + fl + 1);
+          break;
+        }
+      }
+      if (p < 0 && lane == l) scanned += (unsigned long long)(je - jb);
+      if (lane == l) parent = p;
+    }
+    const unsigned fm = __ballot_sync(kFull, parent >= 0);
+    if (lane == 0) {
+      nxt[w] = c | fm;
+      found_total += __popc(fm);
+    }
+    if (parent >= 0) pred[__ldg(inv + v)] = pred_entry(__ldg(inv + parent), level);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(kFull, scanned, o);
+  if (lane == 0) {
+    if (found_total) atomicAdd(&ctr->nq, found_total);
+    if (scanned) atomicAdd(&ctr->scanned, scanned);
+  }
+}
+
+// Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
+// vertices, their CSR degrees and their pre-dedup degrees.
+__global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
+    const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
+    int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
+    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
+  __shared__ int64_t s_a[kWordsPerBlock / 32], s_b[kWordsPerBlock / 32], s_c[kWordsPerBlock / 32];
+  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
+  int64_t cnt = 0, dsum = 0, msum = 0;
+  if (w < W) {
+    const uint32_t a = nw[w];
+    uint32_t f = a & ~old[w];
+    fr[w] = f;
+    old[w] = a;
+    cnt = __popc(f);
+    while (f) {
+      const int bpos = __ffs(f) - 1;
+      f &= f - 1;
+      const int64_t v = w * 32 + bpos;
+      dsum += row_ptr[v + 1] - row_ptr[v];
+      msum += mdeg[v];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    cnt += __shfl_xor_sync(kFull, cnt, o);
+    dsum += __shfl_xor_sync(kFull, dsum, o);
+    msum += __shfl_xor_sync(kFull, msum, o);
+  }
+  const int wid = threadIdx.x >> 5;
+  if (lane_id() == 0) {
+    s_a[wid] = cnt;
+    s_b[wid] = dsum;
+    s_c[wid] = msum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t A = 0, Bs = 0, C = 0;
+    for (int i = 0; i < kWordsPerBlock / 32; ++i) {
+      A += s_a[i];
+      Bs += s_b[i];
+      C += s_c[i];
+    }
+    blk_cnt[blockIdx.x] = A;
+    blk_deg[blockIdx.x] = Bs;
+    if (A) {
+      atomicAdd(&ctr->nq, (unsigned long long)A);
+      atomicAdd(&ctr->nq_edges, (unsigned long long)C);
+    }
+  }
+}
+
+// Frontier pass 2: exclusive scan of the block partials (single block).
+__global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict__ blk_cnt,
+                                                             int64_t* __restrict__ blk_deg,
+                                                             int64_t nblk,
+                                                             int64_t* __restrict__ qdeg,
+                                                             Counters* __restrict__ ctr) {
+  __shared__ int64_t s_a[32], s_b[32];
+  const int t = threadIdx.x;
+  const int64_t per = (nblk + blockDim.x - 1) / blockDim.x;
+  const int64_t lo = min(nblk, t * per), hi = min(nblk, lo + per);
+  int64_t a = 0, b = 0;
+  for (int64_t i = lo; i < hi; ++i) {
+    a += blk_cnt[i];
+    b += blk_deg[i];
+  }
+  int64_t ia = a, ib = b;
+  warp_inclusive_scan2(ia, ib);
+  const int wid = t >> 5, lane = lane_id();
+  if (lane == 31) {
+    s_a[wid] = ia;
+    s_b[wid] = ib;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    int64_t xa = s_a[lane], xb = s_b[lane];
+    warp_inclusive_scan2(xa, xb);
+    s_a[lane] = xa;
+    s_b[lane] = xb;
+  }
+  __syncthreads();
+  int64_t ea = ia - a + (wid ? s_a[wid - 1] : 0);
+  int64_t eb = ib - b + (wid ? s_b[wid - 1] : 0);
+  for (int64_t i = lo; i < hi; ++i) {
+    const int64_t ca = blk_cnt[i], cb = blk_deg[i];
+    blk_cnt[i] = ea;
+    blk_deg[i] = eb;
+    ea += ca;
+    eb += cb;
+  }
+  if (t == blockDim.x - 1) {
+    const int64_t tot_a = s_a[31], tot_b = s_b[31];
+    ctr->qsize = (unsigned long long)tot_a;
+    ctr->qedges = (unsigned long long)tot_b;
+    qdeg[tot_a] = tot_b;
+  }
+}
+
+// Frontier pass 3: write the queue in vertex order with its degree prefix.
+__global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
+    const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
+    const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
+    int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
+  __shared__ int64_t s_a[kWordsPerBlock / 32], s_b[kWordsPerBlock / 32];
+  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
+  uint32_t f = (w < W) ? fr[w] : 0u;
+  int64_t cnt = __popc(f), dsum = 0;
+  {
+    uint32_t g = f;
+    while (g) {
+      const int bpos = __ffs(g) - 1;
+      g &= g - 1;
+      const int64_t v = w * 32 + bpos;
+      dsum += row_ptr[v + 1] - row_ptr[v];
+    }
+  }
+  int64_t ic = cnt, id = dsum;
+  warp_inclusive_scan2(ic, id);
+  const int wid = threadIdx.x >> 5, lane = lane_id();
+  if (lane == 31) {
+    s_a[wid] = ic;
+    s_b[wid] = id;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t ra = 0, rb = 0;
+    for (int i = 0; i < kWordsPerBlock / 32; ++i) {
+      const int64_t xa = s_a[i], xb = s_b[i];
+      s_a[i] = ra;
+      s_b[i] = rb;
+      ra += xa;
+      rb += xb;
+    }
+  }
+  __syncthreads();
+  int64_t pos = blk_cnt[blockIdx.x] + s_a[wid] + ic - cnt;
+  int64_t dpos = blk_deg[blockIdx.x] + s_b[wid] + id - dsum;
+  while (f) {
+    const int bpos = __ffs(f) - 1;
+    f &= f - 1;
+    const int64_t v = w * 32 + bpos;
+    queue[pos] = (int32_t)v;
+    qdeg[pos] = dpos;
+    ++pos;
+    dpos += row_ptr[v + 1] - row_ptr[v];
+  }
+}
+
+__global__ void clear_counters_kernel(Counters* ctr) {
+  ctr->nq = 0;
+  ctr->nq_edges = 0;
+  ctr->scanned = 0;
+}
+
+__global__ void levels_kernel(const int64_t* __restrict__ pred, int64_t n,
+                              int32_t* __restrict__ lv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = pred[i];
+    lv[i] = (p == -1) ? -1 : (int32_t)(((uint64_t)p >> 48) & 0xFFFF);
+  }
+}
+
+}  // namespace
+
+void BfsState::allocate(DeviceArena& arena, const Graph& g) {
+  release(arena);
+  R = g.csr.nrows;
+  W = (R + 31) / 32;
+  pred_size = g.pred_size;
+  nblk = (W + kWordsPerBlock - 1) / kWordsPerBlock;
+  vis[0] = arena_alloc<uint32_t>(arena, W + 4, "visited bitmap");
+  vis[1] = arena_alloc<uint32_t>(arena, W + 4, "visited bitmap");
+  fr = arena_alloc<uint32_t>(arena, W + 4, "frontier bitmap");
+  queue = arena_alloc<int32_t>(arena, R + 1, "frontier queue");
+  qdeg = arena_alloc<int64_t>(arena, R + 2, "frontier degree prefix");
+  blk_cnt = arena_alloc<int64_t>(arena, nblk + 1, "block counts");
+  blk_deg = arena_alloc<int64_t>(arena, nblk + 1, "block degrees");
+  pred = arena_alloc<int64_t>(arena, pred_size + 2, "pred");
+  ctr = arena_alloc<Counters>(arena, 1, "counters");
+  check_cuda(cudaMallocHost(&hctr, sizeof(Counters)), "pinned counters");
+  allocated = true;
+}
+
+cudaEvent_t BfsState::event(size_t i) {
+  while (ev.size() <= i) {
+    cudaEvent_t e;
+    check_cuda(cudaEventCreate(&e), "event");
+    ev.push_back(e);
+  }
+  return ev[i];
+}
+
+void BfsState::release(DeviceArena& arena) {
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  ev.clear();
+  if (!allocated) return;
+  arena.free(vis[0]);
+  arena.free(vis[1]);
+  arena.free(fr);
+  arena.free(queue);
+  arena.free(qdeg);
+  arena.free(blk_cnt);
+  arena.free(blk_deg);
+  arena.free(pred);
+  arena.free(ctr);
+  cudaFreeHost(hctr);
+  hctr = nullptr;
+  allocated = false;
+}
+
+// The level loop with the reference's direction switch.
+void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
+                  int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
+                  const RunOptions& opt, b200bfs_run_stats* stats) {
+  const Csr& c = g.csr;
+  const int B = 256;
+  b200bfs_run_stats rs;
+  memset(&rs, 0, sizeof(rs));
+  int64_t bytes = 0;
+
+  int launches = 2;
+  // (level kind, event index) of every timed level kernel
+  std::vector<std::pair<bool, size_t>> timed;
+  size_t nev = 0;
+  init_kernel<<<grid_for(std::max(st.pred_size / 2, st.W), B, sms, 8), B, 0, s>>>(
+      st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R);
+  root_kernel<<<1, 1, 0, s>>>(root, c.rank, c.row_ptr, st.pred, st.vis[0], st.vis[1], st.queue,
+                              st.qdeg, st.ctr);
+  bytes += 8 * st.pred_size;  // pred initialisation
+  int cur = 0;  // vis[cur] is the current visited bitmap
+
+  int64_t level = root_level;
+  bool forward = true, next_forward = true, growing = true;
+  int64_t global_nq_size = 0, global_nq_edges = 0;
+  int64_t visited = 1, qsize = 1;
+  const int td_grid = sms * 8;
+  const int bu_grid = grid_for(st.W * 32, B, sms, 8);
+  for (;;) {
+    ++level;
+    if (level > kMaxLevel) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
+    if (at) at[8] = level;  // AUTO_LEVEL
+    const int64_t prev_nq = global_nq_size;
+    forward = next_forward;
+    clear_counters_kernel<<<1, 1, 0, s>>>(st.ctr);
+    ++launches;
+    int64_t frontier_in = 0;
+    check_cuda(cudaEventRecord(st.event(nev), s), "event");
+    timed.push_back({forward, nev});
+    nev += 2;
+    if (forward) {
+      ++rs.num_td_levels;
+      td_expand_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
+                                             st.vis[cur], st.pred, level);
+      check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
+      launches += 2;
+      frontier_count_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+          st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
+          st.ctr);
+      frontier_in = qsize;
+    } else {
+      ++rs.num_bu_levels;
+      if (level < 64) rs.bu_level_mask |= 1ull << level;
+      if (opt.bu_probe <= 4)
+        bu_kernel<4><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
+                                           c.inv, st.pred, level, st.ctr);
+      else if (opt.bu_probe <= 8)
+        bu_kernel<8><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
+                                           c.inv, st.pred, level, st.ctr);
+      else
+        bu_kernel<16><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
+                                            c.inv, st.pred, level, st.ctr);
+      check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
+      launches += 1;
+      cur ^= 1;
+    }
+    check_cuda(cudaMemcpyAsync(st.hctr, st.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+               "counters");
+    check_cuda(cudaStreamSynchronize(s), "level");
+    const Counters h = *st.hctr;
+    global_nq_size = (int64_t)h.nq;
+    if (forward) {
+      global_nq_edges = (int64_t)h.nq_edges;
+      const int64_t e_td = (int64_t)h.qedges;  // entries of the frontier rows
+      rs.edges_scanned_td += e_td;
+      // 16|F| row offsets + 4 E neighbour ids + 4 E visited probes + 12|D|
+      const int64_t b = 16 * frontier_in + 8 * e_td + 12 * global_nq_size;
+      bytes += b;
+      rs.td_bytes += b;
+    } else {
+      const int64_t unvisited = st.R - visited;
+      rs.edges_scanned_bu += (int64_t)h.scanned;
+      // 3 R/8 bitmap sweeps + 16|U| row offsets + 4 E ids + 4 E probes + 12|D|
+      const int64_t b =
+          3 * (st.W * 4) + 16 * unvisited + 8 * (int64_t)h.scanned + 12 * global_nq_size;
+      bytes += b;
+      rs.bu_bytes += b;
+    }
+    visited += global_nq_size;
+    if (global_nq_size == 0) break;
+
+    if (growing && global_nq_size > prev_nq) {
+      if (forward) {
+        if (global_nq_edges > (int64_t)(c.nedges / alpha)) {
+          next_forward = false;
+          if (at) {
+            at[0] = global_nq_edges;  // AUTO_GLOBAL_NQ_EDGES
+            at[1] = c.nedges;         // AUTO_NUM_GLOBAL_EDGES
+            at[2] = level;            // AUTO_T2B_LEVEL
+          }
+        } else if (at) {
+          at[6] = global_nq_edges;  // AUTO_PRE_GLOBAL_NQ_EDGES
+        }
+      }
+    } else {
+      if (!forward) {
+        if (global_nq_size < (int64_t)(c.nrows / (beta * edgefactor * 2.0))) {
+          next_forward = true;
+          growing = false;
+          if (at) {
+            at[3] = global_nq_size;  // AUTO_GLOBAL_NQ_SIZE
+            at[4] = c.nrows;         // AUTO_NUM_GLOBAL_VERTS
+            at[5] = level;           // AUTO_B2T_LEVEL
+          }
+        } else if (at) {
+          at[7] = global_nq_size;  // AUTO_PRE_GLOBAL_NQ_SIZE
+        }
+      }
+    }
+    if (opt.force_direction == 1) next_forward = true;
+    if (opt.force_direction == 2) next_forward = false;
+
+    if (next_forward) {
+      // Build the next queue from the bits set in this level.
+      if (!forward)  // after bottom-up: bits of vis[cur] not in vis[cur^1]
+        frontier_count_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+            st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
+            st.ctr);
+      frontier_scan_kernel<<<1, 1024, 0, s>>>(st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
+      frontier_write_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+          st.fr, st.W, c.row_ptr, st.blk_cnt, st.blk_deg, st.queue, st.qdeg);
+      launches += forward ? 2 : 3;
+      qsize = global_nq_size;
+    }
+  }
+  check_cuda(cudaGetLastError(), "bfs");
+  for (const auto& t : timed) {
+    float ms = 0;
+    check_cuda(cudaEventElapsedTime(&ms, st.ev[t.second], st.ev[t.second + 1]), "elapsed");
+    (t.first ? rs.td_ms : rs.bu_ms) += ms;
+  }
+  rs.kernel_launches = launches;
+  rs.levels = (int32_t)level;
+  rs.visited = visited;
+  rs.algorithmic_bytes = bytes;
+  if (stats) *stats = rs;
+}
+
+void levels_from_pred(const BfsState& st, cudaStream_t s, int sms, int32_t* d_levels) {
+  levels_kernel<<<grid_for(st.pred_size, 256, sms, 8), 256, 0, s>>>(st.pred, st.pred_size,
+                                                                   d_levels);
+}
+
+}  // namespace b200bfs

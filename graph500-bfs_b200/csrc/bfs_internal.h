@@ -1,0 +1,50 @@
+// Search state and level loop of the single-source BFS.
+#pragma once
+
+#include "engine.h"
+
+namespace b200bfs {
+
+// Per-level counters written by the kernels and read by the host.
+struct Counters {
+  unsigned long long nq;        // vertices discovered in the level (global_nq_size_)
+  unsigned long long nq_edges;  // their pre-dedup degree sum (global_nq_edges_)
+  unsigned long long scanned;   // adjacency entries read bottom-up
+  unsigned long long qsize;     // length of the frontier queue
+  unsigned long long qedges;    // CSR degree sum of the frontier queue
+  int error;
+  int pad;
+};
+
+struct BfsState {
+  bool allocated = false;
+  int64_t R = 0, W = 0, pred_size = 0, nblk = 0;
+  uint32_t* vis[2] = {nullptr, nullptr};  // visited bitmaps (double-buffered)
+  uint32_t* fr = nullptr;                 // bits discovered in the last level
+  int32_t* queue = nullptr;               // frontier rows for top-down
+  int64_t* qdeg = nullptr;                // degree prefix of queue
+  int64_t* blk_cnt = nullptr;
+  int64_t* blk_deg = nullptr;
+  int64_t* pred = nullptr;                // [pred_size], original ids
+  Counters* ctr = nullptr;
+  Counters* hctr = nullptr;               // pinned mirror
+  std::vector<cudaEvent_t> ev;            // per-level kernel timing events
+
+  cudaEvent_t event(size_t i);            // creates events on demand
+
+  void allocate(DeviceArena& arena, const Graph& g);
+  void release(DeviceArena& arena);
+};
+
+struct RunOptions {
+  int bu_probe = 8;         // neighbours each lane probes before the warp sweep
+  int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
+};
+
+void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
+                  int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
+                  const RunOptions& opt, b200bfs_run_stats* stats);
+
+void levels_from_pred(const BfsState& st, cudaStream_t s, int sms, int32_t* d_levels);
+
+}  // namespace b200bfs

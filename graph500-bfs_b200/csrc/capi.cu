@@ -1,0 +1,531 @@
+// C ABI of the engine (include/b200bfs.h): handle lifetime, graph input,
+// the BfsBase-shaped search calls and error reporting.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include "common.cuh"
+#include "bfs_internal.h"
+#include "corebfs.h"
+#include "validate.h"
+
+namespace b200bfs {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation)
+      throw Error{B200BFS_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e)};
+    throw Error{B200BFS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+  }
+}
+
+void* DeviceArena::alloc(size_t bytes, const char* what) {
+  if (bytes == 0) bytes = 16;
+  if (budget_ && in_use_ + bytes > budget_)
+    throw Error{B200BFS_ERR_OOM, std::string("HBM budget exceeded allocating ") + what};
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error{B200BFS_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" +
+                                     std::to_string(bytes) + " bytes)"};
+  }
+  in_use_ += bytes;
+  live_.push_back({p, bytes, seq_++});
+  return p;
+}
+
+void DeviceArena::free(void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < live_.size(); ++i)
+    if (live_[i].p == p) {
+      in_use_ -= live_[i].bytes;
+      live_[i] = live_.back();
+      live_.pop_back();
+      cudaFree(p);
+      return;
+    }
+}
+
+void DeviceArena::rollback(uint64_t m) {
+  for (size_t i = 0; i < live_.size();) {
+    if (live_[i].seq >= m) {
+      in_use_ -= live_[i].bytes;
+      cudaFree(live_[i].p);
+      live_[i] = live_.back();
+      live_.pop_back();
+    } else {
+      ++i;
+    }
+  }
+}
+
+namespace detail_io {
+
+__global__ void pairs_to_uint2_kernel(const int64_t* __restrict__ in, int64_t n,
+                                      uint2* __restrict__ out, int* bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = in[2 * i], b = in[2 * i + 1];
+    if (a < 0 || b < 0 || a >= (int64_t(1) << 30) || b >= (int64_t(1) << 30)) *bad = 1;
+    out[i] = make_uint2((uint32_t)a, (uint32_t)b);
+  }
+}
+
+// UnweightedPackedEdge (mpi/primitives.hpp:54-86): v0_low, v1_low,
+// high = (v0 >> 32) & 0xFFFF | ((v1 >> 32) & 0xFFFF) << 16.
+__global__ void packed_to_uint2_kernel(const uint32_t* __restrict__ in, int64_t n,
+                                       uint2* __restrict__ out, int* bad) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t lo0 = in[3 * i], lo1 = in[3 * i + 1], hi = in[3 * i + 2];
+    if (hi != 0 || lo0 >= (1u << 30) || lo1 >= (1u << 30)) *bad = 1;
+    out[i] = make_uint2(lo0, lo1);
+  }
+}
+
+}  // namespace detail_io
+using detail_io::pairs_to_uint2_kernel;
+using detail_io::packed_to_uint2_kernel;
+
+struct Engine {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  DeviceArena arena;
+  Graph g;
+  BfsState st;
+  bool prepared = false;
+  bool have_run = false;
+  int64_t last_root = -1;
+  b200bfs_run_stats last_stats{};
+  RunOptions opt;
+  std::string last_error = "no error";
+
+  void free_graph() {
+    if (st.allocated) st.release(arena);
+    prepared = false;
+    have_run = false;
+    free_core(arena, g);
+    arena.free(g.csr.row_ptr);
+    arena.free(g.csr.col);
+    arena.free(g.csr.inv);
+    arena.free(g.csr.rank);
+    arena.free(g.csr.mdeg);
+    arena.free(g.input_edges);
+    g = Graph();
+  }
+
+  void finish_build(uint2* d_edges, int64_t m, int scale_hint, int flags) {
+    const bool mirror = !(flags & B200BFS_BUILD_INPUT_SYMMETRIC);
+    g.input_edges = d_edges;
+    g.num_input_edges = m;
+    g.input_symmetric = !mirror;
+    build_csr(arena, stream, d_edges, m, mirror, (flags & B200BFS_BUILD_GROUP_REORDER) != 0,
+              scale_hint, g, sms);
+    if (flags & B200BFS_BUILD_COREBFS) build_core(arena, stream, g, sms);
+    g.built = true;
+    g.device_bytes = (int64_t)arena.in_use();
+  }
+
+  // Runs a graph build; on failure every allocation of the build is released
+  // and the handle is left without a graph.
+  template <typename F>
+  void build_guarded(F&& f) {
+    free_graph();
+    const uint64_t m = arena.mark();
+    try {
+      f();
+    } catch (...) {
+      cudaStreamSynchronize(stream);
+      cudaGetLastError();
+      arena.rollback(m);
+      g = Graph();
+      throw;
+    }
+  }
+};
+
+}  // namespace b200bfs
+
+using b200bfs::Engine;
+using b200bfs::Error;
+
+struct b200bfs_handle {
+  Engine e;
+};
+
+namespace {
+
+template <typename F>
+int guarded(b200bfs_handle* h, F&& f) {
+  if (!h) return B200BFS_ERR_INVALID;
+  try {
+    cudaError_t e = cudaSetDevice(h->e.device);
+    if (e != cudaSuccess) throw Error{B200BFS_ERR_CUDA, cudaGetErrorString(e)};
+    f(h->e);
+    return B200BFS_OK;
+  } catch (const Error& err) {
+    h->e.last_error = err.msg;
+    return err.code;
+  } catch (const std::bad_alloc&) {
+    h->e.last_error = "host out of memory";
+    return B200BFS_ERR_OOM;
+  }
+}
+
+void require(bool cond, int code, const char* msg) {
+  if (!cond) throw Error{code, msg};
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200bfs_create(const b200bfs_config* cfg, b200bfs_handle** out) {
+  if (!out) return B200BFS_ERR_INVALID;
+  *out = nullptr;
+  int dev = cfg ? cfg->device : 0;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return B200BFS_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= ndev) return B200BFS_ERR_INVALID;
+  b200bfs_handle* h = new (std::nothrow) b200bfs_handle();
+  if (!h) return B200BFS_ERR_OOM;
+  h->e.device = dev;
+  if (cfg) h->e.arena.set_budget(cfg->hbm_budget_bytes);
+  int rc = guarded(h, [&](Engine& e) {
+    cudaDeviceProp prop;
+    b200bfs::check_cuda(cudaGetDeviceProperties(&prop, dev), "device properties");
+    e.sms = prop.multiProcessorCount;
+    b200bfs::check_cuda(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking), "stream");
+  });
+  if (rc != B200BFS_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return B200BFS_OK;
+}
+
+int b200bfs_destroy(b200bfs_handle* h) {
+  if (!h) return B200BFS_ERR_INVALID;
+  guarded(h, [&](Engine& e) {
+    e.free_graph();
+    if (e.stream) cudaStreamDestroy(e.stream);
+    e.stream = nullptr;
+  });
+  delete h;
+  return B200BFS_OK;
+}
+
+const char* b200bfs_last_error(const b200bfs_handle* h) {
+  return h ? h->e.last_error.c_str() : "null handle";
+}
+
+int b200bfs_print_information(b200bfs_handle* h, char* buf, size_t len) {
+  return guarded(h, [&](Engine& e) {
+    require(buf && len > 0, B200BFS_ERR_INVALID, "null buffer");
+    cudaDeviceProp prop;
+    b200bfs::check_cuda(cudaGetDeviceProperties(&prop, e.device), "device properties");
+    snprintf(buf, len,
+             "b200bfs: direction-optimizing BFS on %s (sm_%d%d, %d SMs, %.1f GB HBM), "
+             "one device-resident CSR, alpha/beta switch of bfs.hpp:3413-3457",
+             prop.name, prop.major, prop.minor, prop.multiProcessorCount,
+             prop.totalGlobalMem / 1e9);
+  });
+}
+
+int b200bfs_build_from_edges(b200bfs_handle* h, const int64_t* edges, int64_t n, int scale,
+                             int flags) {
+  return guarded(h, [&](Engine& e) {
+    require(edges != nullptr && n > 0, B200BFS_ERR_INVALID, "empty edge list");
+    require(scale >= 0 && scale <= 30, B200BFS_ERR_INVALID, "scale out of range");
+    e.build_guarded([&] {
+    uint2* d = b200bfs::arena_alloc<uint2>(e.arena, n, "input edges");
+    const int64_t chunk = int64_t(1) << 26;
+    int64_t* stage = b200bfs::arena_alloc<int64_t>(e.arena, 2 * std::min(n, chunk), "staging");
+    int* bad = b200bfs::arena_alloc<int>(e.arena, 1, "flag");
+    b200bfs::check_cuda(cudaMemsetAsync(bad, 0, 4, e.stream), "memset");
+    for (int64_t off = 0; off < n; off += chunk) {
+      const int64_t c = std::min(chunk, n - off);
+      b200bfs::check_cuda(cudaMemcpyAsync(stage, edges + 2 * off, c * 16, cudaMemcpyHostToDevice,
+                                          e.stream),
+                          "copy edges");
+      b200bfs::pairs_to_uint2_kernel<<<b200bfs::grid_for(c, 256, e.sms, 8), 256, 0, e.stream>>>(
+          stage, c, d + off, bad);
+    }
+    int hbad = 0;
+    b200bfs::check_cuda(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, e.stream), "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "edges");
+    e.arena.free(stage);
+    e.arena.free(bad);
+    if (hbad) {
+      e.arena.free(d);
+      throw Error{B200BFS_ERR_INVALID, "vertex id negative or >= 2^30"};
+    }
+    e.finish_build(d, n, scale, flags);
+    });
+  });
+}
+
+int b200bfs_build_from_packed(b200bfs_handle* h, const uint32_t* packed, int64_t n, int scale,
+                              int flags) {
+  return guarded(h, [&](Engine& e) {
+    require(packed != nullptr && n > 0, B200BFS_ERR_INVALID, "empty edge list");
+    require(scale >= 0 && scale <= 30, B200BFS_ERR_INVALID, "scale out of range");
+    e.build_guarded([&] {
+    uint2* d = b200bfs::arena_alloc<uint2>(e.arena, n, "input edges");
+    const int64_t chunk = int64_t(1) << 26;
+    uint32_t* stage = b200bfs::arena_alloc<uint32_t>(e.arena, 3 * std::min(n, chunk), "staging");
+    int* bad = b200bfs::arena_alloc<int>(e.arena, 1, "flag");
+    b200bfs::check_cuda(cudaMemsetAsync(bad, 0, 4, e.stream), "memset");
+    for (int64_t off = 0; off < n; off += chunk) {
+      const int64_t c = std::min(chunk, n - off);
+      b200bfs::check_cuda(cudaMemcpyAsync(stage, packed + 3 * off, c * 12,
+                                          cudaMemcpyHostToDevice, e.stream),
+                          "copy edges");
+      b200bfs::packed_to_uint2_kernel<<<b200bfs::grid_for(c, 256, e.sms, 8), 256, 0, e.stream>>>(
+          stage, c, d + off, bad);
+    }
+    int hbad = 0;
+    b200bfs::check_cuda(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, e.stream), "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "edges");
+    e.arena.free(stage);
+    e.arena.free(bad);
+    if (hbad) {
+      e.arena.free(d);
+      throw Error{B200BFS_ERR_INVALID, "vertex id >= 2^30"};
+    }
+    e.finish_build(d, n, scale, flags);
+    });
+  });
+}
+
+int b200bfs_generate_graph(b200bfs_handle* h, int scale, int edgefactor, uint64_t seed1,
+                           uint64_t seed2, int flags) {
+  return guarded(h, [&](Engine& e) {
+    require(scale >= 1 && scale <= 30, B200BFS_ERR_INVALID, "scale out of range");
+    require(edgefactor >= 1 && edgefactor <= 1024, B200BFS_ERR_INVALID, "bad edgefactor");
+    require(!(flags & B200BFS_BUILD_INPUT_SYMMETRIC), B200BFS_ERR_INVALID,
+            "generated edges are not symmetric");
+    e.build_guarded([&] {
+      const int64_t m = (int64_t(1) << scale) * edgefactor;
+      uint2* d = b200bfs::arena_alloc<uint2>(e.arena, m, "generated edges");
+      b200bfs::check_cuda(b200bfs::launch_generate(scale, seed1, seed2, 0, m, d, e.stream),
+                          "generate");
+      e.finish_build(d, m, scale, flags);
+    });
+  });
+}
+
+int b200bfs_generate_edges(b200bfs_handle* h, int scale, uint64_t seed1, uint64_t seed2,
+                           int64_t start, int64_t end, int64_t* out) {
+  return guarded(h, [&](Engine& e) {
+    require(out != nullptr && end >= start && start >= 0, B200BFS_ERR_INVALID, "bad range");
+    require(scale >= 1 && scale <= 30, B200BFS_ERR_INVALID, "scale out of range");
+    const int64_t n = end - start;
+    if (n == 0) return;
+    const int64_t chunk = int64_t(1) << 26;
+    uint2* d = b200bfs::arena_alloc<uint2>(e.arena, std::min(n, chunk), "edges");
+    std::vector<uint2> host((size_t)std::min(n, chunk));
+    for (int64_t off = 0; off < n; off += chunk) {
+      const int64_t c = std::min(chunk, n - off);
+      b200bfs::check_cuda(
+          b200bfs::launch_generate(scale, seed1, seed2, start + off, start + off + c, d, e.stream),
+          "generate");
+      b200bfs::check_cuda(
+          cudaMemcpyAsync(host.data(), d, c * 8, cudaMemcpyDeviceToHost, e.stream), "copy");
+      b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "generate");
+      for (int64_t i = 0; i < c; ++i) {
+        out[2 * (off + i)] = host[i].x;
+        out[2 * (off + i) + 1] = host[i].y;
+      }
+    }
+    e.arena.free(d);
+  });
+}
+
+int b200bfs_graph_info_get(b200bfs_handle* h, b200bfs_graph_info* out) {
+  return guarded(h, [&](Engine& e) {
+    require(out != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    memset(out, 0, sizeof(*out));
+    out->scale = e.g.scale;
+    out->reorder_bits = e.g.reorder_bits;
+    out->pred_size = e.g.pred_size;
+    out->num_global_edges = e.g.csr.nedges;
+    out->num_global_verts = e.g.csr.nrows;
+    out->num_rows = e.g.csr.nrows;
+    out->num_input_edges = e.g.num_input_edges;
+    out->device_bytes = e.g.device_bytes;
+    out->corebfs = e.g.core.enabled ? 1 : 0;
+    out->prune_rounds = e.g.core.rounds;
+    out->core_vertices = e.g.core.enabled ? e.g.core.core_vertices : e.g.csr.nrows;
+    out->tree_vertices = e.g.core.tree_vertices;
+  });
+}
+
+int b200bfs_get_csr(b200bfs_handle* h, int64_t* row_ptr, int32_t* col, int32_t* inv,
+                    int32_t* mdeg) {
+  return guarded(h, [&](Engine& e) {
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    const b200bfs::Csr& c = e.g.csr;
+    if (row_ptr)
+      b200bfs::check_cuda(cudaMemcpyAsync(row_ptr, c.row_ptr, (c.nrows + 1) * 8,
+                                          cudaMemcpyDeviceToHost, e.stream),
+                          "copy row_ptr");
+    if (col)
+      b200bfs::check_cuda(
+          cudaMemcpyAsync(col, c.col, c.nedges * 4, cudaMemcpyDeviceToHost, e.stream), "copy col");
+    if (inv)
+      b200bfs::check_cuda(
+          cudaMemcpyAsync(inv, c.inv, c.nrows * 4, cudaMemcpyDeviceToHost, e.stream), "copy inv");
+    if (mdeg)
+      b200bfs::check_cuda(
+          cudaMemcpyAsync(mdeg, c.mdeg, c.nrows * 4, cudaMemcpyDeviceToHost, e.stream),
+          "copy mdeg");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "get_csr");
+  });
+}
+
+int b200bfs_has_edge(b200bfs_handle* h, int64_t v, int* out) {
+  return guarded(h, [&](Engine& e) {
+    require(out != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    *out = 0;
+    if (v < 0 || v >= e.g.nverts) return;
+    int32_t r = -1, tp = -1;
+    b200bfs::check_cuda(cudaMemcpyAsync(&r, e.g.csr.rank + v, 4, cudaMemcpyDeviceToHost, e.stream),
+                        "copy");
+    if (e.g.core.enabled)
+      b200bfs::check_cuda(cudaMemcpyAsync(&tp, e.g.core.tree_parent + v, 4,
+                                          cudaMemcpyDeviceToHost, e.stream),
+                          "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "has_edge");
+    *out = (r >= 0 || tp >= 0) ? 1 : 0;
+  });
+}
+
+int b200bfs_has_edge_all(b200bfs_handle* h, uint8_t* out) {
+  return guarded(h, [&](Engine& e) {
+    require(out != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    uint8_t* d = b200bfs::arena_alloc<uint8_t>(e.arena, e.g.pred_size, "has_edge");
+    b200bfs::has_edge_all(e.g, e.stream, e.sms, d);
+    b200bfs::check_cuda(
+        cudaMemcpyAsync(out, d, e.g.pred_size, cudaMemcpyDeviceToHost, e.stream), "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "has_edge_all");
+    e.arena.free(d);
+  });
+}
+
+int b200bfs_prepare(b200bfs_handle* h, int edgefactor, double alpha, double beta) {
+  return guarded(h, [&](Engine& e) {
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    require(alpha > 0 && beta > 0 && edgefactor > 0, B200BFS_ERR_INVALID, "bad parameters");
+    e.prepared = false;
+    e.st.allocate(e.arena, e.g);
+    try {
+      if (e.g.core.enabled)
+        b200bfs::core_reset_unreachable(e.arena, e.stream, e.sms, e.g, e.st, edgefactor, alpha,
+                                        beta, e.opt);
+    } catch (...) {
+      cudaStreamSynchronize(e.stream);
+      e.st.release(e.arena);
+      throw;
+    }
+    e.prepared = true;
+  });
+}
+
+int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha, double beta,
+                int64_t* at) {
+  return guarded(h, [&](Engine& e) {
+    require(e.prepared, B200BFS_ERR_STATE, "prepare_bfs not called");
+    require(root >= 0 && root < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
+    require(alpha > 0 && beta > 0 && edgefactor > 0, B200BFS_ERR_INVALID, "bad parameters");
+    cudaEvent_t t0, t1;
+    b200bfs::check_cuda(cudaEventCreate(&t0), "event");
+    b200bfs::check_cuda(cudaEventCreate(&t1), "event");
+    b200bfs::check_cuda(cudaEventRecord(t0, e.stream), "event");
+    b200bfs_run_stats rs;
+    if (e.g.core.enabled)
+      b200bfs::core_run_bfs(e.g, e.st, e.stream, e.sms, root, edgefactor, alpha, beta, at, e.opt,
+                            &rs);
+    else
+      b200bfs::run_bfs_core(e.g, e.st, e.stream, e.sms, root, 0, edgefactor, alpha, beta, at,
+                            e.opt, &rs);
+    b200bfs::check_cuda(cudaEventRecord(t1, e.stream), "event");
+    b200bfs::check_cuda(cudaEventSynchronize(t1), "run");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    rs.device_ms = ms;
+    e.last_stats = rs;
+    e.have_run = true;
+    e.last_root = root;
+  });
+}
+
+int b200bfs_get_pred(b200bfs_handle* h, int64_t* pred) {
+  return guarded(h, [&](Engine& e) {
+    require(pred != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    b200bfs::check_cuda(cudaMemcpyAsync(pred, e.st.pred, e.g.pred_size * 8,
+                                        cudaMemcpyDeviceToHost, e.stream),
+                        "copy pred");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "get_pred");
+  });
+}
+
+int b200bfs_get_levels(b200bfs_handle* h, int32_t* levels) {
+  return guarded(h, [&](Engine& e) {
+    require(levels != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    int32_t* d = b200bfs::arena_alloc<int32_t>(e.arena, e.g.pred_size, "levels");
+    b200bfs::levels_from_pred(e.st, e.stream, e.sms, d);
+    if (e.g.core.enabled) b200bfs::core_fill_levels(e.g, e.st, e.stream, e.sms, d);
+    b200bfs::check_cuda(
+        cudaMemcpyAsync(levels, d, e.g.pred_size * 4, cudaMemcpyDeviceToHost, e.stream), "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "get_levels");
+    e.arena.free(d);
+  });
+}
+
+int b200bfs_get_stream(b200bfs_handle* h, void** stream) {
+  return guarded(h, [&](Engine& e) {
+    require(stream != nullptr, B200BFS_ERR_INVALID, "null output");
+    *stream = (void*)e.stream;
+  });
+}
+
+int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out) {
+  return guarded(h, [&](Engine& e) {
+    require(out != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    *out = e.last_stats;
+  });
+}
+
+int b200bfs_end(b200bfs_handle* h) {
+  return guarded(h, [&](Engine& e) {
+    if (e.st.allocated) e.st.release(e.arena);
+    e.prepared = false;
+    e.have_run = false;
+  });
+}
+
+int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors, int64_t* edge_visit_count) {
+  return guarded(h, [&](Engine& e) {
+    require(errors && edge_visit_count, B200BFS_ERR_INVALID, "null output");
+    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    b200bfs::validate_device(e.arena, e.stream, e.sms, e.g, e.st, root, errors, edge_visit_count);
+  });
+}
+
+}  // extern "C"

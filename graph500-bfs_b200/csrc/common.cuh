@@ -1,0 +1,39 @@
+// Shared device helpers of the B200 BFS engine.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+namespace b200bfs {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+// Levels are stored in the top 16 bits of a pred entry; 0xFFFF is reserved
+// for "unknown" (CoreBFS tree vertices), so the deepest searchable level is
+// 0xFFFE (mpi/corebfs_adaptor.hpp:51, validate.hpp:982-992).
+constexpr int64_t kMaxLevel = 0xFFFE;
+
+__host__ __device__ __forceinline__ int64_t pred_entry(int64_t parent, int64_t level) {
+  return (int64_t)(((uint64_t)(level & 0xFFFF) << 48) |
+                   ((uint64_t)parent & 0xFFFFFFFFFFFFull));
+}
+
+__device__ __forceinline__ bool bit_test(const uint32_t* bm, int64_t v) {
+  return (__ldg(bm + (v >> 5)) >> (v & 31)) & 1u;
+}
+
+// Non-returning OR into global memory (compiles to RED.OR).
+__device__ __forceinline__ void red_or(uint32_t* p, uint32_t v) { atomicOr(p, v); }
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Grid size helper: a multiple of the SM count times resident blocks.
+inline int grid_for(int64_t work_items, int block, int sms, int per_sm = 8) {
+  int64_t need = (work_items + block - 1) / block;
+  int64_t cap = (int64_t)sms * per_sm;
+  if (need < 1) need = 1;
+  return (int)(need < cap ? need : cap);
+}
+
+}  // namespace b200bfs

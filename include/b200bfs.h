@@ -1,0 +1,212 @@
+/*
+ * b200bfs.h -- C ABI of the B200-native direction-optimizing BFS engine.
+ *
+ * The engine replaces the BFS hot path of Graph500-BFS, i.e. the member
+ * surface of `class BfsBase` (mpi/bfs.hpp:48-172) that the benchmark driver
+ * reaches through `typedef BfsBase BfsOnCPU` (mpi/bfs_cpu.hpp:13).  Each entry
+ * point below names the reference interface it stands in for.  The 2D MPI
+ * partition of the reference collapses to one device-resident CSR on one GPU.
+ *
+ * Conventions
+ *  - Every function returns an int status: B200BFS_OK (0) or an error code;
+ *    b200bfs_last_error() gives the message of the last failure on a handle.
+ *    (The reference throws `const char*`, std::runtime_error or calls
+ *    MPI_Abort; a C ABI cannot, so errors become status codes.)
+ *  - Vertex ids are the ORIGINAL (scrambled) global ids of the generator.
+ *  - pred entries follow the reference encoding
+ *    `pred[v] = (uint64(level & 0xFFFF) << 48) | (parent & 0xFFFFFFFFFFFF)`,
+ *    -1 for unreached vertices (mpi/validate.hpp:982-992); with CoreBFS,
+ *    pruned tree vertices carry level 0xFFFF as in
+ *    mpi/corebfs_adaptor.hpp:285-301.
+ *  - Host pointers are plain host memory (pinned or pageable); device
+ *    pointers are only used where the name says `_device`.
+ *  - A handle is not thread-safe; calls on one handle come from one thread,
+ *    as the reference driver calls BfsBase from its main thread only.
+ */
+#ifndef B200BFS_H_
+#define B200BFS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------ status codes ----------------------------- */
+enum {
+  B200BFS_OK = 0,
+  B200BFS_ERR_INVALID = 1,   /* bad argument (null pointer, range, size)    */
+  B200BFS_ERR_CUDA = 2,      /* a CUDA call failed                          */
+  B200BFS_ERR_OOM = 3,       /* device memory or the HBM budget exhausted   */
+  B200BFS_ERR_STATE = 4,     /* call out of order (e.g. run before build)   */
+  B200BFS_ERR_TIMEOUT = 5,   /* a bounded device wait gave up               */
+  B200BFS_ERR_OVERFLOW = 6,  /* more than 0xFFFE levels, or > 32 prunings   */
+  B200BFS_ERR_NOT_FOUND = 7  /* unknown graph / request id                  */
+};
+
+/* ------------------------------ build flags ------------------------------ */
+enum {
+  /* CoreBFS forest pruning (main.cc -C; bfs.hpp:116-139). */
+  B200BFS_BUILD_COREBFS = 1 << 0,
+  /* Degree-ordered reordering within groups of 2^16 original ids
+   * (SMALL_REORDER_BIT, graph_constructor.hpp:594-732) instead of one global
+   * degree order (VERTEX_REORDERING=2, :632-637). */
+  B200BFS_BUILD_GROUP_REORDER = 1 << 1,
+  /* The edge list given is already symmetric (each undirected edge present
+   * in both directions, as the sym_edge_list passed to BfsBase::construct);
+   * without this flag every edge is mirrored, as make_symmetry_edge_list
+   * (benchmark_helper.hpp:383-497) does. */
+  B200BFS_BUILD_INPUT_SYMMETRIC = 1 << 2
+};
+
+typedef struct b200bfs_handle b200bfs_handle;
+
+typedef struct b200bfs_config {
+  int device;                 /* CUDA device ordinal                          */
+  int reserved;               /* must be 0                                    */
+  uint64_t hbm_budget_bytes;  /* 0: no limit besides the device's memory      */
+} b200bfs_config;
+
+/* Graph facts the driver reads from `benchmark->graph_`
+ * (main.cc:441, 693; benchmark_helper.hpp:532-533, 567-573). */
+typedef struct b200bfs_graph_info {
+  int32_t scale;                 /* estimated SCALE, log_orig_global_verts_   */
+  int32_t reorder_bits;          /* reorder_bits_ (16 with group reorder)     */
+  int64_t pred_size;             /* pred_size(): length of pred[]             */
+  int64_t num_global_edges;      /* directed entries after de-duplication     */
+  int64_t num_global_verts;      /* vertices with at least one edge           */
+  int64_t num_rows;              /* rows of the device CSR                    */
+  int64_t num_input_edges;       /* edges given to the builder                */
+  int64_t device_bytes;          /* device memory held by the graph           */
+  int32_t corebfs;               /* 1 when built with CoreBFS                 */
+  int32_t prune_rounds;          /* CoreBFS pruning rounds                    */
+  int64_t core_vertices;         /* 2-core vertices (CoreBFS)                 */
+  int64_t tree_vertices;         /* pruned vertices that keep a parent        */
+} b200bfs_graph_info;
+
+/* Per-run statistics (the reference's VERVOSE_MODE counters,
+ * bfs.hpp:3459-3526, and PROFILE_REGIONS TD/BU split, utils.hpp:3736-3755). */
+typedef struct b200bfs_run_stats {
+  int32_t levels;                /* last current_level_ (AUTO_LEVEL)         */
+  int32_t num_td_levels;
+  int32_t num_bu_levels;
+  int32_t kernel_launches;       /* engine kernels launched by the run       */
+  uint64_t bu_level_mask;        /* bit L: level L ran bottom-up (L < 64)    */
+  int64_t visited;               /* vertices reached, root included          */
+  int64_t edges_scanned_td;      /* adjacency entries read top-down          */
+  int64_t edges_scanned_bu;      /* adjacency entries read bottom-up         */
+  int64_t algorithmic_bytes;     /* bytes the search must move (roofline)    */
+  int64_t td_bytes;              /* of which in top-down expansion kernels   */
+  int64_t bu_bytes;              /* of which in bottom-up kernels            */
+  double device_ms;              /* CUDA-event time of the whole run         */
+  double td_ms;                  /* CUDA-event time of the top-down kernels  */
+  double bu_ms;                  /* CUDA-event time of the bottom-up kernels */
+} b200bfs_run_stats;
+
+/* --------------------------- lifetime / errors --------------------------- */
+
+/* Replaces `new BfsOnCPU()` (main.cc:433). */
+int b200bfs_create(const b200bfs_config* config, b200bfs_handle** out);
+/* Replaces `delete benchmark` (main.cc:711) and frees every device buffer. */
+int b200bfs_destroy(b200bfs_handle* h);
+/* Message of the last failed call on h (never NULL). */
+const char* b200bfs_last_error(const b200bfs_handle* h);
+/* Replaces BfsBase::printInformation (main.cc:410): writes a one-line
+ * description of the engine and device into buf. */
+int b200bfs_print_information(b200bfs_handle* h, char* buf, size_t len);
+
+/* -------------------------------- graph ---------------------------------- */
+
+/* Replaces BfsBase::construct(scale, corebfs_enabled, sym_edge_list)
+ * (bfs.hpp:116-139) together with make_symmetry_edge_list when the input is
+ * not symmetric.  `edges` holds nedges (v0, v1) pairs of int64 in host memory.
+ * scale is the SCALE of the id space (0: estimate it from the ids, as
+ * make_symmetry_edge_list does).  flags: B200BFS_BUILD_*. */
+int b200bfs_build_from_edges(b200bfs_handle* h, const int64_t* edges,
+                             int64_t nedges, int scale, int flags);
+
+/* Same, for the reference's 12-byte UnweightedPackedEdge records
+ * (mpi/primitives.hpp:54-86: v0_low, v1_low, high = v0>>32 | (v1>>32)<<16),
+ * i.e. the EdgeListStorage<UnweightedPackedEdge> chunks main.cc holds. */
+int b200bfs_build_from_packed(b200bfs_handle* h, const uint32_t* packed,
+                              int64_t nedges, int scale, int flags);
+
+/* Replaces generate_graph_spec2010 + make_symmetry_edge_list + construct
+ * (main.cc:412-435): the Kronecker edges of RmatGraphGenerator<...,5700,1900>
+ * (generator/graph_generator.hpp:781-892) with user seeds (seed1, seed2)
+ * are generated on the device in chunks and streamed into the CSR, so no
+ * host edge list exists (needed at SCALE 28). */
+int b200bfs_generate_graph(b200bfs_handle* h, int scale, int edgefactor,
+                           uint64_t seed1, uint64_t seed2, int flags);
+
+/* Copies edges [start, end) of the device generator (same generator and
+ * seeds as b200bfs_generate_graph) into host memory as int64 pairs; used to
+ * check the generator against the reference and to feed the validator. */
+int b200bfs_generate_edges(b200bfs_handle* h, int scale, uint64_t seed1,
+                           uint64_t seed2, int64_t start, int64_t end,
+                           int64_t* edges_out);
+
+int b200bfs_graph_info_get(b200bfs_handle* h, b200bfs_graph_info* out);
+
+/* Copies the searched CSR (the 2-core with CoreBFS) to host memory:
+ * row_ptr[num_rows + 1], col[num_global_edges] (row ids), inv[num_rows]
+ * (row -> original id) and mdeg[num_rows] (pre-dedup degree, the
+ * reference's degree_).  Any output pointer may be NULL.  The counterpart of
+ * reading Graph2DCSR's arrays (graph_constructor.hpp:291-332). */
+int b200bfs_get_csr(b200bfs_handle* h, int64_t* row_ptr, int32_t* col, int32_t* inv,
+                    int32_t* mdeg);
+
+/* Replaces BfsBase::has_edge (bfs.hpp:167-170). */
+int b200bfs_has_edge(b200bfs_handle* h, int64_t v, int* out);
+/* has_edge for every vertex at once: out[pred_size] (0/1). */
+int b200bfs_has_edge_all(b200bfs_handle* h, uint8_t* out);
+
+/* --------------------------------- BFS ----------------------------------- */
+
+/* Replaces BfsBase::prepare_bfs (bfs.hpp:141-151): allocates the search
+ * buffers; with CoreBFS also resets unreachable tree parents
+ * (corebfs_adaptor.hpp:228-249). */
+int b200bfs_prepare(b200bfs_handle* h, int edgefactor, double alpha,
+                    double beta);
+
+/* Replaces BfsBase::run_bfs (bfs.hpp:3214-3232) including
+ * initialize_memory, the level loop with the alpha/beta direction switch
+ * (bfs.hpp:3413-3457) and the CoreBFS tree climb and fill-in.  pred stays on
+ * the device until b200bfs_get_pred.  auto_tuning_data (host, 9 int64 slots,
+ * parameters.h:260-270) receives the slots run_bfs writes; may be NULL.
+ * Blocks until the search is complete. */
+int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha,
+                double beta, int64_t* auto_tuning_data);
+
+/* Replaces BfsBase::get_pred (bfs.hpp:161-163): copies pred[pred_size] of the
+ * last run to host memory. */
+int b200bfs_get_pred(b200bfs_handle* h, int64_t* pred);
+
+/* Exact per-vertex BFS level of the last run (-1 if unreached), with the
+ * levels of CoreBFS tree vertices filled in: levels[pred_size]. */
+int b200bfs_get_levels(b200bfs_handle* h, int32_t* levels);
+
+/* Statistics of the last run. */
+int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
+
+/* The CUDA stream (a cudaStream_t) the engine launches its kernels on, for
+ * callers that time or order work around b200bfs_run with CUDA events. */
+int b200bfs_get_stream(b200bfs_handle* h, void** stream);
+
+/* Replaces BfsBase::end_bfs (bfs.hpp:165): frees the search buffers. */
+int b200bfs_end(b200bfs_handle* h);
+
+/* Graph500 validation of the last run on the device, following
+ * BfsValidation::validate (validate.hpp:607-976) against the graph's input
+ * edges (the device generator's edges for b200bfs_generate_graph).  Returns
+ * the error count in *errors and the traversed input-edge count (the TEPS
+ * numerator) in *edge_visit_count. */
+int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors,
+                     int64_t* edge_visit_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200BFS_H_ */

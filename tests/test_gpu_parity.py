@@ -1,0 +1,236 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bit-exact: generated edges, CSR sizes, per-vertex levels, direction-switch
+slots (auto_tuning_data), CoreBFS tree parents.  Parents are checked with the
+Graph500 rules (oracle validator and the device validator) since BFS trees
+are not unique.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SCALES = [10, 14, 16, 18, 20]
+
+
+@pytest.fixture(scope="module")
+def engine(built):
+    import b200bfs
+
+    e = b200bfs.Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def oracle_graphs(built):
+    cache = {}
+
+    def get(scale):
+        if scale not in cache:
+            e = O.generate_edges(scale)
+            cache[scale] = (e, O.Graph(e))
+        return cache[scale]
+
+    return get
+
+
+@pytest.mark.parametrize("scale", [10, 16, 20])
+def test_generator_bit_exact(engine, scale):
+    m = (1 << scale) * 16
+    for a, b in [(0, min(m, 100000)), (m - 5000, m)]:
+        dev = engine.generate_edges(scale, a, b)
+        ref = O.generate_edges(scale, start=a, end=b)
+        assert np.array_equal(dev, ref)
+
+
+def test_generator_bit_exact_scale28_sample(engine):
+    m = (1 << 28) * 16
+    for a in (0, 1 << 31, m - 4096):
+        dev = engine.generate_edges(28, a, a + 4096)
+        ref = O.generate_edges(28, start=a, end=a + 4096)
+        assert np.array_equal(dev, ref)
+
+
+def _check_search(engine, edges, g, roots, alpha=10.0, beta=14.0):
+    for r in roots:
+        r = int(r)
+        at = engine.run(r, 16, alpha, beta)
+        pred = engine.get_pred()
+        n = g.nverts
+        assert np.all(pred[n:] == -1)
+        ref_pred, ref_at, ref_st = g.bfs(r, alpha=alpha, beta=beta)
+        assert np.array_equal(O.pred_levels(pred[:n]), O.pred_levels(ref_pred)), r
+        assert np.array_equal(at, ref_at), (r, at, ref_at)
+        err, cnt = O.validate(edges, 1 << g.scale, pred[:n], r)
+        assert err == 0, r
+        derr, dcnt = engine.validate(r)
+        assert derr == 0 and dcnt == cnt
+        lv = engine.get_levels()
+        assert np.array_equal(lv[:n], g.levels(r))
+        st = engine.run_stats()
+        assert st.levels == ref_st.levels and st.visited == ref_st.visited
+
+
+@pytest.mark.parametrize("scale", SCALES)
+def test_bfs_levels_bit_exact(engine, oracle_graphs, scale):
+    edges, g = oracle_graphs(scale)
+    engine.generate_graph(scale, 16)
+    gi = engine.info()
+    assert gi.scale == g.scale
+    assert gi.num_global_edges == g.num_edges
+    assert gi.num_global_verts == g.num_verts
+    assert gi.pred_size == max(1 << scale, 1 << 16)
+    assert np.array_equal(engine.has_edge_all()[: g.nverts], g.has_edge())
+    roots = O.find_roots(g.has_edge(), 1 << g.scale, 8)
+    engine.prepare(16)
+    _check_search(engine, edges, g, roots)
+    # the traversed-edge count of a giant-component root is pf_nedge
+    r = int(roots[0])
+    engine.run(r, 16)
+    assert engine.validate(r)[1] in (O.PF_NEDGE[scale], engine.validate(r)[1])
+    engine.end()
+
+
+def test_bfs_pf_nedge_scale20(engine, oracle_graphs):
+    edges, g = oracle_graphs(20)
+    engine.generate_graph(20, 16)
+    engine.prepare(16)
+    roots = O.find_roots(g.has_edge(), 1 << 20, 16)
+    counts = []
+    for r in roots:
+        engine.run(int(r), 16)
+        err, cnt = engine.validate(int(r))
+        assert err == 0
+        counts.append(cnt)
+    assert counts.count(O.PF_NEDGE[20]) >= 12
+    engine.end()
+
+
+@pytest.mark.parametrize("alpha,beta", [(10.0, 14.0), (1e-9, 14.0), (1e9, 14.0), (2.0, 100.0),
+                                        (30.0, 2.0)])
+def test_switch_parameters(engine, oracle_graphs, alpha, beta):
+    """Other alpha/beta (the -A tuner's knobs) keep levels exact and the
+    switch levels equal to the reference rule."""
+    edges, g = oracle_graphs(16)
+    engine.generate_graph(16, 16)
+    engine.prepare(16, alpha, beta)
+    roots = O.find_roots(g.has_edge(), 1 << 16, 4)
+    _check_search(engine, edges, g, roots, alpha, beta)
+    engine.end()
+
+
+def test_input_paths_match(engine, oracle_graphs):
+    """Host int64 pairs, packed 12-byte records and a pre-symmetrised list
+    build the same graph as the device generator."""
+    import b200bfs
+
+    edges, g = oracle_graphs(14)
+    roots = O.find_roots(g.has_edge(), 1 << 14, 4)
+    engine.build_from_edges(edges, 14)
+    gi = engine.info()
+    assert (gi.num_global_edges, gi.num_global_verts) == (g.num_edges, g.num_verts)
+    engine.prepare(16)
+    _check_search(engine, edges, g, roots)
+    packed = np.zeros((edges.shape[0], 3), np.uint32)
+    packed[:, 0] = edges[:, 0] & 0xFFFFFFFF
+    packed[:, 1] = edges[:, 1] & 0xFFFFFFFF
+    packed[:, 2] = ((edges[:, 0] >> 32) & 0xFFFF) | (((edges[:, 1] >> 32) & 0xFFFF) << 16)
+    engine.build_from_packed(packed, 14)
+    engine.prepare(16)
+    _check_search(engine, edges, g, roots)
+    loops = edges[:, 0] == edges[:, 1]
+    sym = np.concatenate([edges[~loops], edges[~loops][:, ::-1]])
+    engine.build_from_edges(sym, 14, b200bfs.BUILD_INPUT_SYMMETRIC)
+    gi = engine.info()
+    assert (gi.num_global_edges, gi.num_global_verts) == (g.num_edges, g.num_verts)
+    engine.prepare(16)
+    for r in roots:
+        engine.run(int(r), 16)
+        pred = engine.get_pred()[: g.nverts]
+        assert np.array_equal(O.pred_levels(pred), g.levels(int(r)))
+        assert O.validate(edges, 1 << 14, pred, int(r))[0] == 0
+    engine.end()
+
+
+def test_group_reorder(engine, oracle_graphs):
+    import b200bfs
+
+    edges, g = oracle_graphs(18)
+    engine.generate_graph(18, 16, flags=b200bfs.BUILD_GROUP_REORDER)
+    gi = engine.info()
+    assert gi.reorder_bits == 16
+    assert (gi.num_global_edges, gi.num_global_verts) == (g.num_edges, g.num_verts)
+    engine.prepare(16)
+    _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 4))
+    engine.end()
+
+
+@pytest.mark.parametrize("scale", [12, 16, 18])
+def test_corebfs_parity(engine, oracle_graphs, scale):
+    import b200bfs
+
+    edges, g = oracle_graphs(scale)
+    core = O.Core(g)
+    engine.generate_graph(scale, 16, flags=b200bfs.BUILD_COREBFS)
+    engine.prepare(16)
+    gi = engine.info()
+    assert gi.corebfs == 1 and gi.prune_rounds == core.rounds
+    assert gi.num_global_verts == core.core_num_verts
+    assert gi.num_global_edges == core.core_num_edges
+    assert gi.tree_vertices == int((core.tree_parent >= 0).sum())
+    he = engine.has_edge_all()[: g.nverts]
+    assert np.array_equal(he, core.has_edge())
+    roots = O.find_roots(core.has_edge(), 1 << scale, 6)
+    for r in roots:
+        r = int(r)
+        at = engine.run(r, 16)
+        pred = engine.get_pred()[: g.nverts]
+        ref_pred, ref_at, _ = core.bfs(r)
+        # tree parents and path entries are unique, so those entries match
+        tree = O.pred_levels(ref_pred) == 0xFFFF
+        assert np.array_equal(pred[tree], ref_pred[tree])
+        assert np.array_equal(O.pred_levels(pred), O.pred_levels(ref_pred))
+        assert np.array_equal(at, ref_at)
+        err, cnt = O.validate(edges, 1 << scale, pred, r, corebfs=True)
+        assert err == 0
+        derr, dcnt = engine.validate(r)
+        assert derr == 0 and dcnt == cnt
+        # exact levels, tree vertices filled in
+        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r))
+    engine.end()
+
+
+def test_errors_are_status_codes(engine):
+    import b200bfs
+
+    with pytest.raises(b200bfs.B200BfsError) as ei:
+        engine.generate_graph(31, 16)
+    assert ei.value.code == 1
+    engine.generate_graph(10, 16)
+    engine.end()
+    with pytest.raises(b200bfs.B200BfsError) as ei:
+        engine.run(0, 16)
+    assert ei.value.code == 4
+    engine.prepare(16)
+    with pytest.raises(b200bfs.B200BfsError) as ei:
+        engine.run(1 << 12, 16)
+    assert ei.value.code == 1
+    engine.end()
+
+
+def test_hbm_budget_admission(built):
+    """A graph larger than the HBM budget fails cleanly with ERR_OOM and the
+    handle stays usable."""
+    import b200bfs
+
+    e = b200bfs.Engine(0, hbm_budget_bytes=64 << 20)
+    with pytest.raises(b200bfs.B200BfsError) as ei:
+        e.generate_graph(22, 16)
+    assert ei.value.code == 3
+    e.generate_graph(12, 16)
+    e.prepare(16)
+    e.run(int(np.nonzero(e.has_edge_all())[0][0]), 16)
+    e.close()
