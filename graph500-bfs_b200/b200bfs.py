@@ -36,7 +36,7 @@ SYMBOLS = [
     "b200bfs_create", "b200bfs_destroy", "b200bfs_last_error", "b200bfs_print_information",
     "b200bfs_build_from_edges", "b200bfs_build_from_packed", "b200bfs_generate_graph",
     "b200bfs_generate_edges", "b200bfs_graph_info_get", "b200bfs_get_csr", "b200bfs_has_edge",
-    "b200bfs_has_edge_all", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
+    "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_validate",
 ]
@@ -102,6 +102,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_get_csr.argtypes = [H, vp, vp, vp, vp]
     L.b200bfs_has_edge.argtypes = [H, i64, P(ctypes.c_int)]
     L.b200bfs_has_edge_all.argtypes = [H, vp]
+    L.b200bfs_find_roots.argtypes = [H, i32, i32, i32, vp]
     L.b200bfs_prepare.argtypes = [H, i32, dbl, dbl]
     L.b200bfs_run.argtypes = [H, i64, i32, dbl, dbl, vp]
     L.b200bfs_get_pred.argtypes = [H, vp]
@@ -194,6 +195,11 @@ class Engine:
     def has_edge_all(self):
         out = np.empty(self.info().pred_size, dtype=np.uint8)
         self.check(self.L.b200bfs_has_edge_all(self.h, _ptr(out)))
+        return out
+
+    def find_roots(self, num_roots, r1=0, r2=0):
+        out = np.empty(num_roots, dtype=np.int64)
+        self.check(self.L.b200bfs_find_roots(self.h, num_roots, r1, r2, _ptr(out)))
         return out
 
     def prepare(self, edgefactor=16, alpha=DEFAULT_ALPHA, beta=DEFAULT_BETA):

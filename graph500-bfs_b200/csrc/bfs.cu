@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) td_expand_kernel(
     for (int k = 0; k < kTdTile / 32; ++k) {
       const int64_t e = t0 + k * 32 + lane;
       if (e >= total) break;
-      while (e >= seg_hi) {
+      while (e >= seg_hi && i + 1 < qsize) {
         ++i;
         seg_lo = seg_hi;
         seg_hi = qdeg[i + 1];

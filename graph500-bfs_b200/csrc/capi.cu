@@ -423,6 +423,21 @@ int b200bfs_has_edge_all(b200bfs_handle* h, uint8_t* out) {
   });
 }
 
+int b200bfs_find_roots(b200bfs_handle* h, int num_roots, int r1, int r2, int64_t* roots) {
+  return guarded(h, [&](Engine& e) {
+    require(roots != nullptr && num_roots > 0, B200BFS_ERR_INVALID, "bad root buffer");
+    require(e.g.built, B200BFS_ERR_STATE, "no graph built");
+    std::vector<uint8_t> has((size_t)e.g.pred_size);
+    uint8_t* d = b200bfs::arena_alloc<uint8_t>(e.arena, e.g.pred_size, "has_edge");
+    b200bfs::has_edge_all(e.g, e.stream, e.sms, d);
+    b200bfs::check_cuda(
+        cudaMemcpyAsync(has.data(), d, e.g.pred_size, cudaMemcpyDeviceToHost, e.stream), "copy");
+    b200bfs::check_cuda(cudaStreamSynchronize(e.stream), "find_roots");
+    e.arena.free(d);
+    b200bfs::find_roots_host(has.data(), int64_t(1) << e.g.scale, num_roots, r1, r2, roots);
+  });
+}
+
 int b200bfs_prepare(b200bfs_handle* h, int edgefactor, double alpha, double beta) {
   return guarded(h, [&](Engine& e) {
     require(e.g.built, B200BFS_ERR_STATE, "no graph built");

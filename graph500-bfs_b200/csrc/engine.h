@@ -17,6 +17,9 @@ void host_seed_state(uint64_t s1, uint64_t s2, uint32_t z[5]);
 void host_mrg_skip(uint32_t z[5], uint64_t hi, uint64_t mid, uint64_t lo);
 uint32_t host_mrg_next(uint32_t z[5]);
 void host_scramble_values(uint64_t s1, uint64_t s2, uint64_t* v0, uint64_t* v1);
+double host_random_double(uint64_t s1, uint64_t s2, int64_t position);
+void find_roots_host(const uint8_t* has_edge, int64_t nglobal, int num_roots, int r1, int r2,
+                     int64_t* roots);
 
 // Error carrying a status code and message through the engine.
 struct Error {

@@ -206,6 +206,51 @@ void host_scramble_values(uint64_t s1, uint64_t s2, uint64_t* v0, uint64_t* v1) 
   *v1 = b;
 }
 
+// make_random_numbers (graph_generator.hpp:506-520): two MRG outputs per
+// double, (2^31-1)^-1 and (2^31-1)^-2 weights (splittable_mrg.c:330-337).
+double host_random_double(uint64_t s1, uint64_t s2, int64_t position) {
+  uint32_t z[5];
+  host_seed_state(s1, s2, z);
+  host_mrg_skip(z, 2, 0, 2 * (uint64_t)position);
+  const double a = (double)host_mrg_next(z) * 4.656612875245796924105750827e-10;
+  const double b = (double)host_mrg_next(z) * 2.168404346990492787e-19;
+  return a + b;
+}
+
+// find_roots (mpi/benchmark_helper.hpp:527-562) with USERSEED1/2 = 2/3: the
+// counter advances by two doubles per candidate; duplicates and vertices
+// without edges are skipped; after 2*nglobalverts candidates the last one is
+// taken as is.
+void find_roots_host(const uint8_t* has_edge, int64_t nglobal, int num_roots, int r1, int r2,
+                     int64_t* roots) {
+  int64_t counter = 0;
+  for (int idx = 0; idx < num_roots; ++idx) {
+    int64_t root = 0;
+    for (;;) {
+      uint32_t z[5];
+      host_seed_state(2 + (uint64_t)r1, 3 + (uint64_t)r2, z);
+      host_mrg_skip(z, 2, 0, 2 * (uint64_t)counter);
+      const double d0a = (double)host_mrg_next(z) * 4.656612875245796924105750827e-10;
+      const double d0b = (double)host_mrg_next(z) * 2.168404346990492787e-19;
+      const double d1a = (double)host_mrg_next(z) * 4.656612875245796924105750827e-10;
+      const double d1b = (double)host_mrg_next(z) * 2.168404346990492787e-19;
+      const double d0 = d0a + d0b, d1 = d1a + d1b;
+      root = (int64_t)((d0 + d1) * (double)nglobal) % nglobal;
+      counter += 2;
+      if (counter > 2 * nglobal) break;
+      bool dup = false;
+      for (int i = 0; i < idx; ++i)
+        if (roots[i] == root) {
+          dup = true;
+          break;
+        }
+      if (dup) continue;
+      if (has_edge[root]) break;
+    }
+    roots[idx] = root;
+  }
+}
+
 cudaError_t launch_generate(int scale, uint64_t seed1, uint64_t seed2, int64_t start, int64_t end,
                             uint2* out, cudaStream_t stream) {
   // The tables are re-sent on every call: constant memory is per device and

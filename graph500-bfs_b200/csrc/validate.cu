@@ -82,7 +82,7 @@ __global__ void depth_build_kernel(int64_t* __restrict__ pred, int64_t n, int64_
   }
 }
 
-__global__ void edge_check_kernel(const uint2* __restrict__ edges, int64_t m,
+__global__ void edge_check_kernel(const uint2* __restrict__ edges, int64_t m, int64_t n,
                                   const int64_t* __restrict__ pred, uint8_t* __restrict__ valid,
                                   unsigned long long* err, unsigned long long* count) {
   unsigned long long e = 0, c = 0;
@@ -90,6 +90,10 @@ __global__ void edge_check_kernel(const uint2* __restrict__ edges, int64_t m,
        i += (int64_t)gridDim.x * blockDim.x) {
     const uint2 ed = edges[i];
     const int64_t s = ed.x, t = ed.y;
+    if (s >= n || t >= n) {  // endpoint outside pred[]
+      ++e;
+      continue;
+    }
     const int64_t ps = pred[s], pt = pred[t];
     const int sd = depth_of(ps), td = depth_of(pt);
     if (sd != 0xFFFF && td == 0xFFFF) ++e;
@@ -180,8 +184,8 @@ void validate_device(DeviceArena& arena, cudaStream_t s, int sms, const Graph& g
     }
     uint8_t* valid = arena_alloc<uint8_t>(arena, n, "pred valid");
     check_cuda(cudaMemsetAsync(valid, 0, n, s), "memset");
-    edge_check_kernel<<<grid(g.num_input_edges), B, 0, s>>>(g.input_edges, g.num_input_edges, p,
-                                                            valid, cnt, cnt + 1);
+    edge_check_kernel<<<grid(g.num_input_edges), B, 0, s>>>(g.input_edges, g.num_input_edges, n,
+                                                            p, valid, cnt, cnt + 1);
     parent_edge_kernel<<<grid(n), B, 0, s>>>(p, n, root, valid, cnt);
     unsigned long long h2[2] = {0, 0};
     check_cuda(cudaMemcpyAsync(h2, cnt, 16, cudaMemcpyDeviceToHost, s), "copy");

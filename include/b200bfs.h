@@ -162,6 +162,11 @@ int b200bfs_has_edge(b200bfs_handle* h, int64_t v, int* out);
 /* has_edge for every vertex at once: out[pred_size] (0/1). */
 int b200bfs_has_edge_all(b200bfs_handle* h, uint8_t* out);
 
+/* find_roots (mpi/benchmark_helper.hpp:527-562): the driver's search-key
+ * sampler with user seeds (2 + r1, 3 + r2) over has_edge; writes num_roots
+ * vertex ids.  main.cc calls it with r1 = root seed (+1 per re-pick), r2 = 0. */
+int b200bfs_find_roots(b200bfs_handle* h, int num_roots, int r1, int r2, int64_t* roots);
+
 /* --------------------------------- BFS ----------------------------------- */
 
 /* Replaces BfsBase::prepare_bfs (bfs.hpp:141-151): allocates the search

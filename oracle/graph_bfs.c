@@ -108,165 +108,35 @@ void orc_graph_free(orc_graph* g) {
 
 #define BIT_TEST(bm, v) (((bm)[(v) >> 6] >> ((v)&63)) & 1)
 
-/* Direction-optimizing BFS restating BfsBase::run_bfs_core
- * (mpi/bfs.hpp:3238-3609) on one rank:
- *  - initialize_memory (:315-349): pred = -1, visited = ~has_edge;
- *  - first_expand (:562-631): pred[root] = root at level 0;
- *  - top-down (:1355-1418 + receive :1420-1693): claim unvisited neighbours
- *    of the frontier, pred = parent | level << 48; nq_edges sums the
- *    pre-dedup degree of the new frontier (:1377-1390);
- *  - bottom-up (:2184-2414, :3007-3059): each unvisited vertex with edges
- *    scans its neighbours in order and takes the first one visited before this
- *    level, which is a vertex of the previous level;
- *  - switch rule and auto_tuning_data slots (:3413-3457).
- */
+#define BFS_NAME bfs_impl64
+#define COL_T int64_t
+#define MDEG_T int64_t
+#include "bfs_body.inc"
+#undef BFS_NAME
+#undef COL_T
+#undef MDEG_T
+#define BFS_NAME bfs_impl32
+#define COL_T int32_t
+#define MDEG_T int32_t
+#include "bfs_body.inc"
+#undef BFS_NAME
+#undef COL_T
+#undef MDEG_T
+
 int orc_bfs(const orc_graph* g, int64_t root, int64_t root_level,
             int edgefactor, double alpha, double beta, int64_t* pred,
             int64_t* at, orc_bfs_stats* stats) {
-  const int64_t n = g->nverts;
-  const int64_t words = (n + 63) / 64;
-  uint64_t* vis = (uint64_t*)calloc(words, 8);
-  uint64_t* vis_old = (uint64_t*)calloc(words, 8);
-  uint64_t* nqbm = (uint64_t*)calloc(words, 8);
-  int64_t* cq = (int64_t*)malloc((n + 1) * sizeof(int64_t));
-  int64_t* nq = (int64_t*)malloc((n + 1) * sizeof(int64_t));
-  int64_t cq_size = 0, nq_size = 0;
-  orc_bfs_stats st;
-  memset(&st, 0, sizeof(st));
+  return bfs_impl64(g->nverts, g->row_ptr, g->col, g->multideg, g->num_edges,
+                    g->num_verts, NULL, g->nverts, root, root_level, edgefactor,
+                    alpha, beta, pred, at, stats);
+}
 
-#pragma omp parallel for
-  for (int64_t i = 0; i < n; ++i) pred[i] = -1;
-#pragma omp parallel for
-  for (int64_t w = 0; w < words; ++w) {
-    uint64_t has = 0;
-    for (int b = 0; b < 64; ++b) {
-      int64_t v = w * 64 + b;
-      if (v < n && g->row_ptr[v + 1] > g->row_ptr[v]) has |= UINT64_C(1) << b;
-    }
-    vis[w] = ~has;
-  }
-
-  int64_t level = root_level;
-  pred[root] = root;
-  vis[root >> 6] |= UINT64_C(1) << (root & 63);
-  cq[0] = root;
-  cq_size = 1;
-  st.visited = 1;
-
-  int forward = 1, next_forward = 1, growing = 1;
-  int64_t global_nq_size = 0, global_nq_edges = 0;
-  for (;;) {
-    at[AUTO_LEVEL] = ++level;
-    const int64_t prev_nq = global_nq_size;
-    forward = next_forward;
-    nq_size = 0;
-    global_nq_edges = 0;
-    if (forward) {
-      int64_t scanned = 0, nq_edges = 0;
-      memset(nqbm, 0, words * 8);
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : scanned)
-      for (int64_t i = 0; i < cq_size; ++i) {
-        const int64_t v = cq[i];
-        for (int64_t j = g->row_ptr[v]; j < g->row_ptr[v + 1]; ++j) {
-          const int64_t u = g->col[j];
-          ++scanned;
-          if (BIT_TEST(vis, u)) continue;
-          uint64_t bit = UINT64_C(1) << (u & 63);
-          uint64_t old = __atomic_fetch_or(&vis[u >> 6], bit, __ATOMIC_RELAXED);
-          if (old & bit) continue;
-          pred[u] = (int64_t)(((uint64_t)level << 48) | (uint64_t)v);
-          __atomic_fetch_or(&nqbm[u >> 6], bit, __ATOMIC_RELAXED);
-        }
-      }
-      for (int64_t w = 0; w < words; ++w) {
-        uint64_t x = nqbm[w];
-        while (x) {
-          int b = __builtin_ctzll(x);
-          x &= x - 1;
-          int64_t u = w * 64 + b;
-          nq[nq_size++] = u;
-          nq_edges += g->multideg[u];
-        }
-      }
-      st.edges_td += scanned;
-      global_nq_edges = nq_edges;
-    } else {
-      if (level < 32) st.direction_mask |= 1u << level;
-      memcpy(vis_old, vis, words * 8);
-      int64_t scanned = 0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : scanned)
-      for (int64_t w = 0; w < words; ++w) {
-        uint64_t todo = ~vis_old[w];
-        uint64_t found = 0;
-        while (todo) {
-          int b = __builtin_ctzll(todo);
-          todo &= todo - 1;
-          int64_t u = w * 64 + b;
-          if (u >= n) break;
-          for (int64_t j = g->row_ptr[u]; j < g->row_ptr[u + 1]; ++j) {
-            const int64_t v = g->col[j];
-            ++scanned;
-            if (BIT_TEST(vis_old, v)) {
-              pred[u] = (int64_t)(((uint64_t)level << 48) | (uint64_t)v);
-              found |= UINT64_C(1) << b;
-              break;
-            }
-          }
-        }
-        vis[w] = vis_old[w] | found;
-      }
-      st.edges_bu += scanned;
-      for (int64_t w = 0; w < words; ++w) {
-        uint64_t x = vis[w] & ~vis_old[w];
-        while (x) {
-          int b = __builtin_ctzll(x);
-          x &= x - 1;
-          nq[nq_size++] = w * 64 + b;
-        }
-      }
-    }
-    global_nq_size = nq_size;
-    st.visited += nq_size;
-    if (global_nq_size == 0) break;
-
-    if (growing && global_nq_size > prev_nq) {
-      if (forward) {
-        if (global_nq_edges > (int64_t)(g->num_edges / alpha)) {
-          next_forward = 0;
-          at[AUTO_GLOBAL_NQ_EDGES] = global_nq_edges;
-          at[AUTO_NUM_GLOBAL_EDGES] = g->num_edges;
-          at[AUTO_T2B_LEVEL] = level;
-        } else {
-          at[AUTO_PRE_GLOBAL_NQ_EDGES] = global_nq_edges;
-        }
-      }
-    } else {
-      if (!forward) {
-        if (global_nq_size <
-            (int64_t)(g->num_verts / (beta * edgefactor * 2.0))) {
-          next_forward = 1;
-          growing = 0;
-          at[AUTO_GLOBAL_NQ_SIZE] = global_nq_size;
-          at[AUTO_NUM_GLOBAL_VERTS] = g->num_verts;
-          at[AUTO_B2T_LEVEL] = level;
-        } else {
-          at[AUTO_PRE_GLOBAL_NQ_SIZE] = global_nq_size;
-        }
-      }
-    }
-    int64_t* t = cq;
-    cq = nq;
-    nq = t;
-    cq_size = nq_size;
-  }
-  st.levels = (int)level;
-  if (stats) *stats = st;
-  free(vis);
-  free(vis_old);
-  free(nqbm);
-  free(cq);
-  free(nq);
-  return 0;
+int orc_bfs_csr32(int64_t nrows, const int64_t* row_ptr, const int32_t* col,
+                  const int32_t* mdeg, const int32_t* inv, int64_t npred,
+                  int64_t root_row, int edgefactor, double alpha, double beta,
+                  int64_t* pred, int64_t* at, orc_bfs_stats* stats) {
+  return bfs_impl32(nrows, row_ptr, col, mdeg, row_ptr[nrows], nrows, inv, npred,
+                    root_row, 0, edgefactor, alpha, beta, pred, at, stats);
 }
 
 int orc_bfs_levels_simple(const orc_graph* g, int64_t root, int32_t* level) {

@@ -102,6 +102,15 @@ int orc_bfs(const orc_graph* g, int64_t root, int64_t root_level,
             int edgefactor, double alpha, double beta, int64_t* pred,
             int64_t* auto_tuning_data, orc_bfs_stats* stats);
 
+/* The same search over an int32-column CSR whose rows are renumbered
+ * vertices (the engine's CSR copied to host memory): row r is original vertex
+ * inv[r]; pred[npred] is written in original ids.  Used as the timed CPU
+ * restatement of the reference's search on the benchmark graph. */
+int orc_bfs_csr32(int64_t nrows, const int64_t* row_ptr, const int32_t* col,
+                  const int32_t* mdeg, const int32_t* inv, int64_t npred,
+                  int64_t root_row, int edgefactor, double alpha, double beta,
+                  int64_t* pred, int64_t* auto_tuning_data, orc_bfs_stats* stats);
+
 /* Per-vertex BFS level with a plain queue BFS (the debugging oracle
  * bfs_local, external/indexed_bfs/bfs/corebfs.hpp:217-261): -1 if unreached. */
 int orc_bfs_levels_simple(const orc_graph* g, int64_t root, int32_t* level);
