@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Graph500 BFS benchmark of the B200 engine.
+
+Metric: harmonic-mean GTEPS of single-source direction-optimizing BFS on the
+Graph500 Kronecker graph (SCALE 28, edgefactor 16, seeds 2/3), the quantity
+main.cc prints as harmonic_mean_TEPS (mpi/main.cc:684-701, logfile.h:86-101):
+TEPS_i = edge_visit_count_i / bfs_time_i, harmonic mean over the roots.
+The graph is generated on the device (synthetic input of the benchmark's own
+generator); roots come from find_roots with the re-pick rule of
+find_roots_in_large_graph (main.cc:334-359); every root's parent array is
+validated on the device before timing and its traversed-edge count is the
+TEPS numerator.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one search from one root (the roots cycle).  N > 1 runs N
+independent replicas (one graph per GPU; the search does not shard), launched
+with torch.distributed.run; times are the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "graph500-bfs_b200"))
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=64)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=28)
+    p.add_argument("--edgefactor", type=int, default=16)
+    p.add_argument("--roots", type=int, default=64)
+    p.add_argument("--root-seed", type=int, default=0)
+    p.add_argument("--alpha", type=float, default=10.0)
+    p.add_argument("--beta", type=float, default=14.0)
+    p.add_argument("--corebfs", action="store_true")
+    p.add_argument("--group-reorder", action="store_true")
+    p.add_argument("--cpu-sample-sec", type=float, default=20.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        d = json.load(open(path))
+        return d.get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def barrier_max(dist, value):
+    """Barrier, then the max of value over ranks."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier_sum(dist, value):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def build_flags(args):
+    import b200bfs
+
+    return (b200bfs.BUILD_COREBFS if args.corebfs else 0) | (
+        b200bfs.BUILD_GROUP_REORDER if args.group_reorder else 0)
+
+
+def pick_roots(eng, args):
+    """find_roots + the re-pick rule of find_roots_in_large_graph
+    (main.cc:334-359): roots are drawn again with the next seed while any of
+    them reaches no more than 3 levels.  Each root's result is validated on
+    the device (validation level 2) and its traversed-edge count kept."""
+    r = args.root_seed
+    while True:
+        roots = eng.find_roots(args.roots, r, 0)
+        nedge, ok = [], True
+        for root in roots:
+            at = eng.run(int(root), args.edgefactor, args.alpha, args.beta)
+            if args.scale > 6 and at[8] <= 3:
+                ok = False
+                break
+            err, cnt = eng.validate(int(root))
+            if err != 0:
+                raise RuntimeError(f"validation failed for root {root}: {err} errors")
+            nedge.append(cnt)
+        if ok:
+            return roots, np.array(nedge, dtype=np.float64)
+        log(f"root seed {r}: a root reaches <= 3 levels, picking roots again")
+        r += 1
+
+
+def harmonic_teps(nedge, times):
+    return len(times) / float(np.sum(np.asarray(times) / np.asarray(nedge)))
+
+
+def cpu_search_sample(row_ptr, col, mdeg, inv, pred_size, rows, nedge, args, budget_sec):
+    """Times the oracle's CPU restatement of the reference search on the
+    benchmark graph for a bounded sample of roots."""
+    import ctypes
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    L = O.lib()
+    L.orc_bfs_csr32.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(O.BfsStats)]
+    pred = np.empty(pred_size, dtype=np.int64)
+    at = np.full(9, -1, dtype=np.int64)
+    st = O.BfsStats()
+    times, used = [], []
+    t_start = time.perf_counter()
+    for i, r in enumerate(rows):
+        t0 = time.perf_counter()
+        L.orc_bfs_csr32(row_ptr.shape[0] - 1, O._ptr(row_ptr), O._ptr(col), O._ptr(mdeg),
+                        O._ptr(inv), pred_size, int(r), args.edgefactor, args.alpha, args.beta,
+                        O._ptr(pred), O._ptr(at), ctypes.byref(st))
+        times.append(time.perf_counter() - t0)
+        used.append(nedge[i])
+        if time.perf_counter() - t_start > budget_sec:
+            break
+    return times, used, O.num_threads()
+
+
+def host_csr(eng):
+    row_ptr, col, inv, mdeg = eng.get_csr()
+    return row_ptr, col, inv, mdeg
+
+
+def rows_of(inv, roots, nverts):
+    """CSR rows of the given original vertex ids."""
+    rank = np.full(nverts, -1, dtype=np.int64)
+    rank[inv] = np.arange(inv.size, dtype=np.int64)
+    return rank[np.asarray(roots, dtype=np.int64)]
+
+
+def workload_config(args):
+    return {"workload": f"Graph500 Kronecker SCALE {args.scale} edgefactor {args.edgefactor} "
+                        f"(A,B,C=.57,.19,.19, seeds 2/3), {args.roots} roots, single-source "
+                        "direction-optimizing BFS",
+            "scale": args.scale, "edgefactor": args.edgefactor, "roots": args.roots,
+            "corebfs": bool(args.corebfs), "group_reorder": bool(args.group_reorder),
+            "alpha": args.alpha, "beta": args.beta,
+            "l2": "inputs larger than L2 (device CSR of tens of GB, pred re-initialised "
+                  "every search)",
+            "parallelism": "replicas"}
+
+
+def run_reference(args, rank, world, dist):
+    """The reference arm: the reference algorithm (CPU restatement in oracle/)
+    on the host cores, same graph, metric and unit."""
+    if rank != 0:
+        return
+    import b200bfs
+
+    t0 = time.time()
+    eng = b200bfs.Engine(0)
+    eng.generate_graph(args.scale, args.edgefactor, flags=build_flags(args))
+    eng.prepare(args.edgefactor, args.alpha, args.beta)
+    roots, nedge = pick_roots(eng, args)
+    info = eng.info()
+    row_ptr, col, inv, mdeg = host_csr(eng)
+    eng.close()
+    log(f"graph ready for the CPU search in {time.time() - t0:.1f}s")
+    rows = rows_of(inv, roots, 1 << info.scale)
+    order = [i % len(rows) for i in range(args.warmup + args.steps)]
+    import ctypes
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    times_w, _, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size,
+                                          rows[order[: args.warmup]], nedge[order[: args.warmup]],
+                                          args, 1e9)
+    steps = order[args.warmup:]
+    times, used, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size, rows[steps],
+                                           nedge[steps], args, 1e9)
+    value = harmonic_teps(used, times) / 1e9
+    line = {
+        "impl": "reference", "metric": f"harmonic-mean GTEPS, SCALE {args.scale}",
+        "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (Graph500 Kronecker generator, seeds 2/3)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
+                         "sample": f"{len(times)} searches at SCALE {args.scale} with the "
+                                   "oracle's OpenMP restatement of BfsBase::run_bfs_core "
+                                   "(graph built on the GPU and copied to host memory)"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, dist = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, rank, world, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    import torch
+    import b200bfs
+
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    eng = b200bfs.Engine(local)
+    eng.generate_graph(args.scale, args.edgefactor, flags=build_flags(args))
+    t_build = time.time() - t0
+    eng.prepare(args.edgefactor, args.alpha, args.beta)
+    info = eng.info()
+    log(f"[rank {rank}] graph: SCALE {info.scale}, {info.num_global_verts} vertices, "
+        f"{info.num_global_edges} directed edges, built in {t_build:.1f}s, "
+        f"{info.device_bytes / 1e9:.1f} GB on device")
+    roots, nedge = pick_roots(eng, args)
+    log(f"[rank {rank}] roots validated; nedge {int(nedge.min())}..{int(nedge.max())}")
+
+    stream = torch.cuda.ExternalStream(eng.stream())
+    order = [i % len(roots) for i in range(args.warmup + args.steps)]
+    for i in order[: args.warmup]:
+        eng.run(int(roots[i]), args.edgefactor, args.alpha, args.beta)
+
+    # ---- timed region: device-resident graph ----
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stats = []
+    for k, i in enumerate(order[args.warmup:]):
+        ev[k][0].record(stream)
+        eng.run(int(roots[i]), args.edgefactor, args.alpha, args.beta)
+        ev[k][1].record(stream)
+        stats.append(eng.run_stats())
+    torch.cuda.synchronize()
+    times = [a.elapsed_time(b) / 1e3 for a, b in ev]
+    used = [nedge[i] for i in order[args.warmup:]]
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    total = barrier_max(dist, sum(times))
+    local_teps = harmonic_teps(used, times)
+    # all replicas process the same roots: whole-job rate = sum over ranks at
+    # the slowest rank's time
+    value = barrier_sum(dist, local_teps * sum(times)) / total / 1e9
+
+    # ---- e2e through the C ABI: search + pred to pinned host memory ----
+    pinned = torch.empty(info.pred_size, dtype=torch.int64, pin_memory=True)
+    pinned_np = pinned.numpy()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k, i in enumerate(order[args.warmup:]):
+        ev2[k][0].record(stream)
+        eng.run(int(roots[i]), args.edgefactor, args.alpha, args.beta)
+        eng.get_pred(pinned_np)
+        ev2[k][1].record(stream)
+    torch.cuda.synchronize()
+    times2 = [a.elapsed_time(b) / 1e3 for a, b in ev2]
+    total2 = barrier_max(dist, sum(times2))
+    e2e = barrier_sum(dist, harmonic_teps(used, times2) * sum(times2)) / total2 / 1e9
+
+    # ---- roofline of the dominant kernel ----
+    td_ms = sum(s.td_ms for s in stats)
+    bu_ms = sum(s.bu_ms for s in stats)
+    if bu_ms >= td_ms:
+        kname, kms, kbytes = "bu_kernel", bu_ms, sum(s.bu_bytes for s in stats)
+        launches = sum(s.num_bu_levels for s in stats)
+    else:
+        kname, kms, kbytes = "td_expand_kernel", td_ms, sum(s.td_bytes for s in stats)
+        launches = sum(s.num_td_levels for s in stats)
+    peak, peak_kind = peaks()
+    achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": ncu_traffic(kname),
+                "algorithmic_bytes_per_launch": kbytes / max(launches, 1),
+                "launches": launches, "share_of_search_time":
+                    kms / (1e3 * sum(times)) if times else None,
+                "whole_search_algorithmic_gbs":
+                    sum(s.algorithmic_bytes for s in stats) / sum(times) / 1e9}
+
+    line = {
+        "metric": f"harmonic-mean GTEPS, SCALE {args.scale}", "value": value, "unit": "GTEPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (Graph500 Kronecker generator on the device, seeds 2/3)",
+        "config": workload_config(args),
+        "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8,
+                "d2h_bytes_per_step": 8 * info.pred_size},
+        "roofline": roofline,
+        "clocks": clk,
+        "gpu_launches": int(barrier_sum(dist, sum(s.kernel_launches for s in stats))),
+        "search": {"edges_scanned_per_input_edge":
+                       float(np.mean([(s.edges_scanned_td + s.edges_scanned_bu) for s in stats]))
+                       / (info.num_input_edges or 1),
+                   "levels": int(np.median([s.levels for s in stats])),
+                   "td_ms": td_ms / args.steps, "bu_ms": bu_ms / args.steps,
+                   "build_s": t_build},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        row_ptr, col, inv, mdeg = host_csr(eng)
+        rows = rows_of(inv, roots, 1 << info.scale)
+        ct, cu, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size, rows, nedge,
+                                          args, args.cpu_sample_sec)
+        line["cpu_baseline"] = {
+            "value": harmonic_teps(cu, ct) / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
+            "sample": f"{len(ct)} searches at SCALE {args.scale} (about {sum(ct):.0f} s) with the "
+                      "oracle's OpenMP restatement of BfsBase::run_bfs_core on the same graph"}
+        del row_ptr, col, inv, mdeg
+    eng.end()
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
