@@ -338,12 +338,14 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     stats = []
+    torch.cuda.nvtx.range_push("bench_timed")
     for k, i in enumerate(order[args.warmup:]):
         ev[k][0].record(stream)
         eng.run(int(roots[i]), args.edgefactor, args.alpha, args.beta)
         ev[k][1].record(stream)
         stats.append(eng.run_stats())
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     times = [a.elapsed_time(b) / 1e3 for a, b in ev]
     used = [nedge[i] for i in order[args.warmup:]]
     if dist is not None:
