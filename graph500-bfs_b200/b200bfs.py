@@ -38,6 +38,7 @@ SYMBOLS = [
     "b200bfs_generate_edges", "b200bfs_graph_info_get", "b200bfs_get_csr", "b200bfs_has_edge",
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
+    "b200bfs_auto_tune",
     "b200bfs_validate",
 ]
 
@@ -105,6 +106,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_find_roots.argtypes = [H, i32, i32, i32, vp]
     L.b200bfs_prepare.argtypes = [H, i32, dbl, dbl]
     L.b200bfs_run.argtypes = [H, i64, i32, dbl, dbl, vp]
+    L.b200bfs_auto_tune.argtypes = [H, vp, i32, vp, i32, P(dbl), P(dbl), P(dbl)]
     L.b200bfs_get_pred.argtypes = [H, vp]
     L.b200bfs_get_levels.argtypes = [H, vp]
     L.b200bfs_get_run_stats.argtypes = [H, P(RunStats)]
@@ -210,6 +212,16 @@ class Engine:
             at = np.full(AUTO_NUM, AUTO_NOT_DEFINED, dtype=np.int64)
         self.check(self.L.b200bfs_run(self.h, int(root), edgefactor, alpha, beta, _ptr(at)))
         return at
+
+    def auto_tune(self, roots, nedge, edgefactor=16, alpha=DEFAULT_ALPHA, beta=DEFAULT_BETA):
+        """The -A tuner (main.cc:361-391); returns (alpha, beta, harmonic TEPS)."""
+        roots = np.ascontiguousarray(roots, dtype=np.int64)
+        nedge = np.ascontiguousarray(nedge, dtype=np.float64)
+        a, b, t = ctypes.c_double(alpha), ctypes.c_double(beta), ctypes.c_double(0)
+        self.check(self.L.b200bfs_auto_tune(self.h, _ptr(roots), roots.size, _ptr(nedge),
+                                            edgefactor, ctypes.byref(a), ctypes.byref(b),
+                                            ctypes.byref(t)))
+        return a.value, b.value, t.value
 
     def get_pred(self, out=None):
         if out is None:

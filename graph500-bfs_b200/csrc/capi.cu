@@ -9,6 +9,7 @@
 #include "bfs_internal.h"
 #include "corebfs.h"
 #include "validate.h"
+#include "autotune.h"
 
 namespace b200bfs {
 
@@ -484,6 +485,55 @@ int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha, d
     e.last_stats = rs;
     e.have_run = true;
     e.last_root = root;
+  });
+}
+
+int b200bfs_auto_tune(b200bfs_handle* h, const int64_t* roots, int num_roots,
+                      const double* nedge, int edgefactor, double* alpha, double* beta,
+                      double* teps) {
+  return guarded(h, [&](Engine& e) {
+    require(roots && nedge && alpha && beta && num_roots > 0, B200BFS_ERR_INVALID,
+            "bad arguments");
+    require(e.prepared, B200BFS_ERR_STATE, "prepare_bfs not called");
+    require(*alpha > 0 && *beta > 0 && edgefactor > 0, B200BFS_ERR_INVALID, "bad parameters");
+    std::vector<int64_t> r(roots, roots + num_roots);
+    std::vector<double> ne(nedge, nedge + num_roots);
+    for (int64_t v : r)
+      require(v >= 0 && v < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
+    auto search = [&](int64_t root, double a, double b, int64_t* at) {
+      b200bfs_run_stats rs;
+      if (e.g.core.enabled)
+        b200bfs::core_run_bfs(e.g, e.st, e.stream, e.sms, root, edgefactor, a, b, at, e.opt, &rs);
+      else
+        b200bfs::run_bfs_core(e.g, e.st, e.stream, e.sms, root, 0, edgefactor, a, b, at, e.opt,
+                              &rs);
+    };
+    // each search is timed with events on the engine stream
+    cudaEvent_t t0, t1;
+    b200bfs::check_cuda(cudaEventCreate(&t0), "event");
+    b200bfs::check_cuda(cudaEventCreate(&t1), "event");
+    b200bfs::SearchFn timed = [&](int64_t root, double a, double b, int64_t* at) {
+      b200bfs::check_cuda(cudaEventRecord(t0, e.stream), "event");
+      search(root, a, b, at);
+      b200bfs::check_cuda(cudaEventRecord(t1, e.stream), "event");
+      b200bfs::check_cuda(cudaEventSynchronize(t1), "event");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, t0, t1);
+      return ms / 1e3;
+    };
+    int tries = 0;
+    double t = 0;
+    try {
+      t = b200bfs::auto_tune(timed, r, ne, edgefactor, alpha, beta, &tries);
+    } catch (...) {
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      throw;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (teps) *teps = t;
+    e.have_run = true;
   });
 }
 

@@ -184,6 +184,17 @@ int b200bfs_prepare(b200bfs_handle* h, int edgefactor, double alpha,
 int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha,
                 double beta, int64_t* auto_tuning_data);
 
+/* The driver's -A mode, auto_tuning of mpi/main.cc:361-391: searches every
+ * root, then moves alpha and afterwards beta one switch level at a time while
+ * the moved root gets faster (auto_tuning_each, main.cc:45-311).  nedge[i] is
+ * the TEPS numerator of roots[i] (the reference uses pf_nedge[SCALE]).
+ * *alpha and *beta are read and tuned in place; *teps (may be NULL) receives
+ * the harmonic-mean TEPS of the final measurement.  Search times are
+ * CUDA-event times of the engine's stream. */
+int b200bfs_auto_tune(b200bfs_handle* h, const int64_t* roots, int num_roots,
+                      const double* nedge, int edgefactor, double* alpha, double* beta,
+                      double* teps);
+
 /* Replaces BfsBase::get_pred (bfs.hpp:161-163): copies pred[pred_size] of the
  * last run to host memory. */
 int b200bfs_get_pred(b200bfs_handle* h, int64_t* pred);
