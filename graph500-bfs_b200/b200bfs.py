@@ -39,7 +39,7 @@ SYMBOLS = [
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_auto_tune",
-    "b200bfs_validate",
+    "b200bfs_validate", "b200bfs_bfs_noalloc",
 ]
 
 
@@ -113,6 +113,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_get_stream.argtypes = [H, P(ctypes.c_void_p)]
     L.b200bfs_end.argtypes = [H]
     L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
+    L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
     _lib = L
     return L
 
@@ -254,6 +255,23 @@ class Engine:
         self.check(self.L.b200bfs_validate(self.h, int(root), ctypes.byref(err),
                                            ctypes.byref(cnt)))
         return err.value, cnt.value
+
+
+NOALLOC_MAX_ROWS = 1 << 24  # B200BFS_NOALLOC_MAX_ROWS
+
+
+def bfs_noalloc(row_ptr_dev, col_dev, nrows, root, pred_dev, stream=0):
+    """b200bfs_bfs_noalloc on device pointers (ints); returns the number of
+    levels.  Searches without allocating device memory (see include/b200bfs.h);
+    raises B200BfsError on a non-zero status."""
+    L = load_library()
+    nl = ctypes.c_int32(0)
+    rc = L.b200bfs_bfs_noalloc(ctypes.c_void_p(row_ptr_dev), ctypes.c_void_p(col_dev), nrows,
+                               root, ctypes.c_void_p(pred_dev), ctypes.c_void_p(stream),
+                               ctypes.byref(nl))
+    if rc != OK:
+        raise B200BfsError(rc, "b200bfs_bfs_noalloc failed")
+    return nl.value
 
 
 class _GraphFacade:

@@ -221,6 +221,30 @@ int b200bfs_end(b200bfs_handle* h);
 int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors,
                      int64_t* edge_visit_count);
 
+/* ------------------------- allocation-free search ------------------------ */
+
+/* Largest graph b200bfs_bfs_noalloc accepts (rows of the CSR). */
+#define B200BFS_NOALLOC_MAX_ROWS (1 << 24)
+
+/* No counterpart in the reference: an entry point for callers that may not
+ * allocate device memory -- code running under CUDA graph capture, programs
+ * whose memory pool owns the whole device, hosts with a fixed budget.  It
+ * searches a CSR the caller already holds on the device (row_ptr[nrows + 1]
+ * int64, col[row_ptr[nrows]] int32 row ids, rows sorted or not) from `root`
+ * and writes pred[nrows] (device memory, same encoding as pred above with row
+ * ids as vertex ids, -1 unreached); *num_levels (host, may be NULL) receives
+ * the last level, as AUTO_LEVEL.  stream is a cudaStream_t (NULL = legacy
+ * default stream); the call returns once the search is complete.
+ * It allocates nothing: its scratch (two visited bitmaps and a counter) lives
+ * in one fixed device array of B200BFS_NOALLOC_MAX_ROWS / 4 bytes that every
+ * GPU loading the library keeps until exit.  Graphs with more rows are
+ * rejected with B200BFS_ERR_INVALID.  The first call on a device looks up
+ * that array's device address, so make it before capturing a stream into a
+ * graph.  All calls share the array: calls that overlap on the GPU (other
+ * threads or streams) race and must be serialised by the caller. */
+int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, int64_t nrows,
+                        int64_t root, int64_t* pred, void* stream, int32_t* num_levels);
+
 #ifdef __cplusplus
 }
 #endif
