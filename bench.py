@@ -377,7 +377,7 @@ def main():
     td_ms = sum(s.td_ms for s in stats)
     bu_ms = sum(s.bu_ms for s in stats)
     if bu_ms >= td_ms:
-        kname, kms, kbytes = "bu_kernel", bu_ms, sum(s.bu_bytes for s in stats)
+        kname, kms, kbytes = "bu_wide_kernel", bu_ms, sum(s.bu_bytes for s in stats)
         launches = sum(s.num_bu_levels for s in stats)
     else:
         kname, kms, kbytes = "td_expand_kernel", td_ms, sum(s.td_bytes for s in stats)

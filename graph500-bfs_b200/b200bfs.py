@@ -38,7 +38,7 @@ SYMBOLS = [
     "b200bfs_generate_edges", "b200bfs_graph_info_get", "b200bfs_get_csr", "b200bfs_has_edge",
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
-    "b200bfs_auto_tune",
+    "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
     "b200bfs_validate", "b200bfs_bfs_noalloc",
 ]
 
@@ -76,6 +76,13 @@ class RunStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class LevelStats(ctypes.Structure):
+    _fields_ = [("level", ctypes.c_int32), ("bottom_up", ctypes.c_int32),
+                ("input", ctypes.c_int64), ("discovered", ctypes.c_int64),
+                ("scanned", ctypes.c_int64), ("algorithmic_bytes", ctypes.c_int64),
+                ("ms", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -111,6 +118,8 @@ def load_library(path=LIB_PATH):
     L.b200bfs_get_levels.argtypes = [H, vp]
     L.b200bfs_get_run_stats.argtypes = [H, P(RunStats)]
     L.b200bfs_get_stream.argtypes = [H, P(ctypes.c_void_p)]
+    L.b200bfs_set_option.argtypes = [H, ctypes.c_char_p, i64]
+    L.b200bfs_get_level_stats.argtypes = [H, vp, i32, P(ctypes.c_int)]
     L.b200bfs_end.argtypes = [H]
     L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
@@ -239,6 +248,18 @@ class Engine:
         rs = RunStats()
         self.check(self.L.b200bfs_get_run_stats(self.h, ctypes.byref(rs)))
         return rs
+
+    def level_stats(self):
+        """Per-level records of the last search, as dicts."""
+        n = ctypes.c_int(0)
+        self.check(self.L.b200bfs_get_level_stats(self.h, None, 0, ctypes.byref(n)))
+        arr = (LevelStats * max(n.value, 1))()
+        self.check(self.L.b200bfs_get_level_stats(self.h, ctypes.cast(arr, ctypes.c_void_p),
+                                                  n.value, ctypes.byref(n)))
+        return [{k: getattr(arr[i], k) for k, _ in LevelStats._fields_} for i in range(n.value)]
+
+    def set_option(self, name, value):
+        self.check(self.L.b200bfs_set_option(self.h, name.encode(), int(value)))
 
     def stream(self):
         """The engine's cudaStream_t as an integer handle."""

@@ -216,6 +216,207 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
   }
 }
 
+// Bottom-up step, second form: a warp step covers kWords bitmap words, so
+// every lane owns kWords vertices and issues their row-offset loads, then
+// their neighbour-id loads (two neighbours per round), then the visited
+// probes, back to back: kWords * 2 independent loads are in flight per lane
+// instead of one dependent chain.  Rows unresolved after 8 probes are swept
+// by the whole warp as in bu_kernel.
+template <int kWords, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
+    const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
+    const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ inv, int64_t* __restrict__ pred, int64_t level,
+    Counters* __restrict__ ctr) {
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long found_total = 0, scanned = 0;
+  for (int64_t w0 = gw * kWords; w0 < W; w0 += nwarps * kWords) {
+    uint32_t c[kWords];
+    bool all_full = true;
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      c[k] = (w0 + k < W) ? cur[w0 + k] : kFull;
+      all_full &= (c[k] == kFull);
+    }
+    if (all_full) {
+      if (lane < kWords && w0 + lane < W) nxt[w0 + lane] = kFull;
+      continue;
+    }
+    int64_t b[kWords], e[kWords];
+    int32_t par[kWords];
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      par[k] = -1;
+      b[k] = e[k] = 0;
+      if (((~c[k]) >> lane) & 1u) {
+        const int64_t v = (w0 + k) * 32 + lane;
+        b[k] = row_ptr[v];
+        e[k] = row_ptr[v + 1];
+      }
+    }
+    // four rounds of two probes per vertex
+#pragma unroll
+    for (int round = 0; round < 4; ++round) {
+      int32_t u0[kWords], u1[kWords];
+      bool need = false;
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) {
+        u0[k] = u1[k] = -1;
+        if (par[k] < 0 && b[k] < e[k]) {
+          u0[k] = __ldg(col + b[k]);
+          if (b[k] + 1 < e[k]) u1[k] = __ldg(col + b[k] + 1);
+          need = true;
+        }
+      }
+      if (!__any_sync(kFull, need)) break;
+      uint32_t m0[kWords], m1[kWords];
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) {
+        m0[k] = u0[k] >= 0 ? __ldg(cur + (u0[k] >> 5)) : 0u;
+        m1[k] = u1[k] >= 0 ? __ldg(cur + (u1[k] >> 5)) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) {
+        if (u0[k] < 0) continue;
+        if ((m0[k] >> (u0[k] & 31)) & 1u) {
+          par[k] = u0[k];
+          scanned += 1;
+        } else if (u1[k] >= 0 && ((m1[k] >> (u1[k] & 31)) & 1u)) {
+          par[k] = u1[k];
+          scanned += 2;
+        } else {
+          scanned += (u1[k] >= 0) ? 2 : 1;
+          b[k] = min(e[k], b[k] + 2);
+        }
+      }
+    }
+    // cooperative sweep of the rows still unresolved
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      unsigned rem = __ballot_sync(kFull, par[k] < 0 && b[k] < e[k]);
+      while (rem) {
+        const int l = __ffs(rem) - 1;
+        rem &= rem - 1;
+        const int64_t jb = __shfl_sync(kFull, b[k], l), je = __shfl_sync(kFull, e[k], l);
+        int32_t p = -1;
+        for (int64_t j = jb; j < je; j += 32) {
+          const int64_t jj = j + lane;
+          int32_t u = 0;
+          bool hit = false;
+          if (jj < je) {
+            u = __ldg(col + jj);
+            hit = bit_test(cur, u);
+          }
+          const unsigned hm = __ballot_sync(kFull, hit);
+          if (hm) {
+            const int fl = __ffs(hm) - 1;
+            p = __shfl_sync(kFull, u, fl);
+            if (lane == l) scanned += (unsigned long long)(j - jb + fl + 1);
+            break;
+          }
+        }
+        if (p < 0 && lane == l) scanned += (unsigned long long)(je - jb);
+        if (lane == l) par[k] = p;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      const unsigned fm = __ballot_sync(kFull, par[k] >= 0);
+      if (lane == 0 && w0 + k < W) {
+        nxt[w0 + k] = c[k] | fm;
+        found_total += __popc(fm);
+      }
+      if (par[k] >= 0) {
+        const int64_t v = (w0 + k) * 32 + lane;
+        pred[__ldg(inv + v)] = pred_entry(__ldg(inv + par[k]), level);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(kFull, scanned, o);
+  if (lane == 0) {
+    if (found_total) atomicAdd(&ctr->nq, found_total);
+    if (scanned) atomicAdd(&ctr->scanned, scanned);
+  }
+}
+
+// Top-down expansion, second form.  The tile's first frontier row is found
+// with a 32-way search (each lane probes one of 32 evenly spaced prefix
+// entries per step), and the tile's eight neighbour ids are loaded before its
+// eight visited probes.
+__global__ void __launch_bounds__(256) td_wide_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  const int64_t qsize = (int64_t)ctr->qsize;
+  if (qsize == 0) return;
+  const int64_t total = qdeg[qsize];
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (total + kTdTile - 1) / kTdTile;
+  constexpr int kPer = kTdTile / 32;
+  for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
+    const int64_t t0 = tile * kTdTile;
+    // Largest i in [0, qsize) with qdeg[i] <= t0.  Invariant: the answer is
+    // in [lo, hi] and qdeg[lo] <= t0 (qdeg[0] = 0), so lane 0 always votes
+    // yes; lanes whose probe lies beyond hi never vote and never load.
+    int64_t lo = 0, hi = qsize - 1;
+    while (hi - lo > 31) {  // more than 32 candidates left
+      const int64_t step = (hi - lo + 31) / 32;
+      const int64_t probe = lo + step * lane;
+      const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t0);
+      const int last = 31 - __clz(le);
+      const int64_t next = lo + step * (last + 1);  // first probe known to be > t0
+      lo += step * last;
+      if (last < 31 && next <= hi) hi = next - 1;
+    }
+    {
+      const int64_t probe = lo + lane;
+      const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t0);
+      lo += 31 - __clz(le);
+    }
+    int64_t i = lo;
+    int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
+    int32_t src = queue[i];
+    int64_t rbeg = row_ptr[src];
+    int32_t srcs[kPer];
+    int32_t us[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int64_t e = t0 + k * 32 + lane;
+      us[k] = -1;
+      srcs[k] = -1;
+      if (e < total) {
+        while (e >= seg_hi && i + 1 < qsize) {
+          ++i;
+          seg_lo = seg_hi;
+          seg_hi = qdeg[i + 1];
+          src = queue[i];
+          rbeg = row_ptr[src];
+        }
+        us[k] = __ldg(col + rbeg + (e - seg_lo));
+        srcs[k] = src;
+      }
+    }
+    uint32_t words[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) words[k] = us[k] >= 0 ? vis[us[k] >> 5] : kFull;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      if (us[k] < 0) continue;
+      const uint32_t bit = 1u << (us[k] & 31);
+      if ((words[k] & bit) == 0) {
+        pred[__ldg(inv + us[k])] = pred_entry(__ldg(inv + srcs[k]), level);
+        red_or(vis + (us[k] >> 5), bit);
+      }
+    }
+  }
+}
+
 // Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
 // vertices, their CSR degrees and their pre-dedup degrees.
 __global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
@@ -453,8 +654,10 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   bool forward = true, next_forward = true, growing = true;
   int64_t global_nq_size = 0, global_nq_edges = 0;
   int64_t visited = 1, qsize = 1;
+  st.levels.clear();
   const int td_grid = sms * 8;
   const int bu_grid = grid_for(st.W * 32, B, sms, 8);
+  const int bu_wide_grid = sms * 8;
   for (;;) {
     ++level;
     if (level > kMaxLevel) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
@@ -469,7 +672,11 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     nev += 2;
     if (forward) {
       ++rs.num_td_levels;
-      td_expand_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
+      if (opt.td_kernel == 1)
+        td_expand_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
+                                               st.vis[cur], st.pred, level);
+      else
+        td_wide_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
                                              st.vis[cur], st.pred, level);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 2;
@@ -480,7 +687,17 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     } else {
       ++rs.num_bu_levels;
       if (level < 64) rs.bu_level_mask |= 1ull << level;
-      if (opt.bu_probe <= 4)
+      if (opt.bu_kernel == 2)
+        bu_wide_kernel<2, 8><<<bu_wide_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
+                                                        c.row_ptr, c.col, c.inv, st.pred, level,
+                                                        st.ctr);
+      else if (opt.bu_kernel == 3)
+        bu_wide_kernel<2, 6><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr,
+                                                   c.col, c.inv, st.pred, level, st.ctr);
+      else if (opt.bu_kernel == 4)
+        bu_wide_kernel<4, 4><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr,
+                                                   c.col, c.inv, st.pred, level, st.ctr);
+      else if (opt.bu_probe <= 4)
         bu_kernel<4><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
                                            c.inv, st.pred, level, st.ctr);
       else if (opt.bu_probe <= 8)
@@ -506,6 +723,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       const int64_t b = 16 * frontier_in + 8 * e_td + 12 * global_nq_size;
       bytes += b;
       rs.td_bytes += b;
+      st.levels.push_back({(int32_t)level, 0, frontier_in, global_nq_size, e_td, b, 0.0});
     } else {
       const int64_t unvisited = st.R - visited;
       rs.edges_scanned_bu += (int64_t)h.scanned;
@@ -514,6 +732,8 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
           3 * (st.W * 4) + 16 * unvisited + 8 * (int64_t)h.scanned + 12 * global_nq_size;
       bytes += b;
       rs.bu_bytes += b;
+      st.levels.push_back(
+          {(int32_t)level, 1, unvisited, global_nq_size, (int64_t)h.scanned, b, 0.0});
     }
     visited += global_nq_size;
     if (global_nq_size == 0) break;
@@ -563,10 +783,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     }
   }
   check_cuda(cudaGetLastError(), "bfs");
-  for (const auto& t : timed) {
+  for (size_t k = 0; k < timed.size(); ++k) {
+    const auto& t = timed[k];
     float ms = 0;
     check_cuda(cudaEventElapsedTime(&ms, st.ev[t.second], st.ev[t.second + 1]), "elapsed");
     (t.first ? rs.td_ms : rs.bu_ms) += ms;
+    if (k < st.levels.size()) st.levels[k].ms = ms;
   }
   rs.kernel_launches = launches;
   rs.levels = (int32_t)level;

@@ -29,6 +29,7 @@ struct BfsState {
   Counters* ctr = nullptr;
   Counters* hctr = nullptr;               // pinned mirror
   std::vector<cudaEvent_t> ev;            // per-level kernel timing events
+  std::vector<b200bfs_level_stats> levels;  // per-level record of the last search
 
   cudaEvent_t event(size_t i);            // creates events on demand
 
@@ -37,7 +38,12 @@ struct BfsState {
 };
 
 struct RunOptions {
-  int bu_probe = 8;         // neighbours each lane probes before the warp sweep
+  // Bottom-up form.  1: bu_kernel (one word per warp step); 2, 3, 4:
+  // bu_wide_kernel with 2 words at 8 or 6 resident CTAs per SM, or 4 words
+  // at 4 per SM.  Form 4 is the fastest measured at SCALE 24 and 28.
+  int bu_kernel = 4;
+  int td_kernel = 1;        // 1: td_expand_kernel, 2: td_wide_kernel
+  int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
 };
 

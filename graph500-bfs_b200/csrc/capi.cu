@@ -562,10 +562,41 @@ int b200bfs_get_levels(b200bfs_handle* h, int32_t* levels) {
   });
 }
 
+int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
+  return guarded(h, [&](Engine& e) {
+    require(name != nullptr, B200BFS_ERR_INVALID, "null option name");
+    const std::string n(name);
+    if (n == "bu_kernel") {
+      require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "bu_kernel must be 1..4");
+      e.opt.bu_kernel = (int)value;
+    } else if (n == "td_kernel") {
+      require(value >= 1 && value <= 2, B200BFS_ERR_INVALID, "td_kernel must be 1..2");
+      e.opt.td_kernel = (int)value;
+    } else if (n == "bu_probe") {
+      require(value >= 1 && value <= 64, B200BFS_ERR_INVALID, "bu_probe must be 1..64");
+      e.opt.bu_probe = (int)value;
+    } else if (n == "force_direction") {
+      require(value >= 0 && value <= 2, B200BFS_ERR_INVALID, "force_direction must be 0..2");
+      e.opt.force_direction = (int)value;
+    } else {
+      throw b200bfs::Error{B200BFS_ERR_INVALID, "unknown option " + n};
+    }
+  });
+}
+
 int b200bfs_get_stream(b200bfs_handle* h, void** stream) {
   return guarded(h, [&](Engine& e) {
     require(stream != nullptr, B200BFS_ERR_INVALID, "null output");
     *stream = (void*)e.stream;
+  });
+}
+
+int b200bfs_get_level_stats(b200bfs_handle* h, b200bfs_level_stats* out, int max, int* count) {
+  return guarded(h, [&](Engine& e) {
+    require(count != nullptr && (out != nullptr || max == 0), B200BFS_ERR_INVALID, "null output");
+    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    *count = (int)e.st.levels.size();
+    for (int i = 0; i < max && i < *count; ++i) out[i] = e.st.levels[(size_t)i];
   });
 }
 

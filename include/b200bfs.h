@@ -104,6 +104,18 @@ typedef struct b200bfs_run_stats {
   double bu_ms;                  /* CUDA-event time of the bottom-up kernels */
 } b200bfs_run_stats;
 
+/* One level of the last search (the per-level report of the reference's
+ * VERVOSE_MODE, bfs.hpp:3459-3526). */
+typedef struct b200bfs_level_stats {
+  int32_t level;                 /* current_level_                           */
+  int32_t bottom_up;             /* 1: bottom-up step, 0: top-down           */
+  int64_t input;                 /* frontier rows (top-down) or unvisited rows (bottom-up) */
+  int64_t discovered;            /* vertices found in the level (NQ)         */
+  int64_t scanned;               /* adjacency entries read                   */
+  int64_t algorithmic_bytes;
+  double ms;                     /* CUDA-event time of the level's kernel    */
+} b200bfs_level_stats;
+
 /* --------------------------- lifetime / errors --------------------------- */
 
 /* Replaces `new BfsOnCPU()` (main.cc:433). */
@@ -203,8 +215,20 @@ int b200bfs_get_pred(b200bfs_handle* h, int64_t* pred);
  * levels of CoreBFS tree vertices filled in: levels[pred_size]. */
 int b200bfs_get_levels(b200bfs_handle* h, int32_t* levels);
 
+/* Per-level records of the last run: up to max entries into out, the
+ * number of levels in *count. */
+int b200bfs_get_level_stats(b200bfs_handle* h, b200bfs_level_stats* out, int max, int* count);
+
 /* Statistics of the last run. */
 int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
+
+/* Engine tuning knobs (no counterpart in the reference, whose equivalents
+ * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
+ * kernel form), "td_kernel" (1..2, top-down kernel form), "bu_probe" (1..64,
+ * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
+ * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2).  None of
+ * them changes levels or the validity of parents. */
+int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value);
 
 /* The CUDA stream (a cudaStream_t) the engine launches its kernels on, for
  * callers that time or order work around b200bfs_run with CUDA events. */

@@ -234,3 +234,20 @@ def test_hbm_budget_admission(built):
     e.prepare(16)
     e.run(int(np.nonzero(e.has_edge_all())[0][0]), 16)
     e.close()
+
+
+@pytest.mark.parametrize("bu,td", [(1, 1), (2, 2), (3, 1), (4, 2)])
+def test_kernel_forms_agree(engine, oracle_graphs, bu, td):
+    """Every bottom-up / top-down kernel form gives the reference levels."""
+    edges, g = oracle_graphs(18)
+    engine.generate_graph(18, 16)
+    engine.set_option("bu_kernel", bu)
+    engine.set_option("td_kernel", td)
+    engine.prepare(16)
+    try:
+        _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 3))
+        _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 2), alpha=1e-9)
+    finally:
+        engine.set_option("bu_kernel", 2)
+        engine.set_option("td_kernel", 2)
+        engine.end()
