@@ -39,8 +39,10 @@ SYMBOLS = [
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
-    "b200bfs_validate", "b200bfs_bfs_noalloc",
+    "b200bfs_validate", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
 ]
+BATCH_MAX = 64  # B200BFS_BATCH_MAX
+BATCH_ALPHA = 30.0  # batch default of the top-down -> bottom-up threshold
 
 
 class B200BfsError(RuntimeError):
@@ -83,6 +85,18 @@ class LevelStats(ctypes.Structure):
                 ("ms", ctypes.c_double)]
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [("num_roots", ctypes.c_int32), ("levels", ctypes.c_int32),
+                ("num_td_levels", ctypes.c_int32), ("num_bu_levels", ctypes.c_int32),
+                ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("edges_scanned_td", ctypes.c_int64), ("edges_scanned_bu", ctypes.c_int64),
+                ("algorithmic_bytes", ctypes.c_int64), ("bu_bytes", ctypes.c_int64),
+                ("ms", ctypes.c_double), ("bu_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 _lib = None
 
 
@@ -123,6 +137,8 @@ def load_library(path=LIB_PATH):
     L.b200bfs_end.argtypes = [H]
     L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
+    L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
+    L.b200bfs_batch_select.argtypes = [H, i32]
     _lib = L
     return L
 
@@ -269,6 +285,19 @@ class Engine:
 
     def end(self):
         self.check(self.L.b200bfs_end(self.h))
+
+    def run_batch(self, roots, edgefactor=16, alpha=BATCH_ALPHA, beta=DEFAULT_BETA):
+        """One multi-source search from up to 64 roots; returns BatchStats."""
+        r = np.ascontiguousarray(np.asarray(roots, dtype=np.int64))
+        bs = BatchStats()
+        self.check(self.L.b200bfs_run_batch(self.h, _ptr(r), len(r), edgefactor, alpha, beta,
+                                            ctypes.byref(bs)))
+        return bs
+
+    def batch_select(self, index):
+        """Makes root `index` of the last batch the current result (pred,
+        levels and validation then refer to it)."""
+        self.check(self.L.b200bfs_batch_select(self.h, int(index)))
 
     def validate(self, root):
         err = ctypes.c_int64()

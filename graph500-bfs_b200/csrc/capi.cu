@@ -10,6 +10,7 @@
 #include "corebfs.h"
 #include "validate.h"
 #include "autotune.h"
+#include "msbfs.h"
 
 namespace b200bfs {
 
@@ -97,6 +98,7 @@ struct Engine {
   DeviceArena arena;
   Graph g;
   BfsState st;
+  BatchState bs;
   bool prepared = false;
   bool have_run = false;
   int64_t last_root = -1;
@@ -106,6 +108,7 @@ struct Engine {
 
   void free_graph() {
     if (st.allocated) st.release(arena);
+    bs.release(arena);
     prepared = false;
     have_run = false;
     free_core(arena, g);
@@ -611,8 +614,36 @@ int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out) {
 int b200bfs_end(b200bfs_handle* h) {
   return guarded(h, [&](Engine& e) {
     if (e.st.allocated) e.st.release(e.arena);
+    e.bs.release(e.arena);
     e.prepared = false;
     e.have_run = false;
+  });
+}
+
+int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, int edgefactor,
+                      double alpha, double beta, b200bfs_batch_stats* stats) {
+  return guarded(h, [&](Engine& e) {
+    require(e.prepared, B200BFS_ERR_STATE, "prepare_bfs not called");
+    require(roots != nullptr && num_roots >= 1 && num_roots <= B200BFS_BATCH_MAX,
+            B200BFS_ERR_INVALID, "num_roots must be 1..64");
+    require(beta > 0 && edgefactor > 0, B200BFS_ERR_INVALID, "bad parameters");
+    for (int i = 0; i < num_roots; ++i)
+      require(roots[i] >= 0 && roots[i] < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
+    b200bfs_batch_stats rs;
+    b200bfs::run_batch(e.arena, e.g, e.st, e.bs, e.stream, e.sms, roots, num_roots, edgefactor,
+                       alpha, beta, &rs);
+    if (stats) *stats = rs;
+    e.have_run = false;
+  });
+}
+
+int b200bfs_batch_select(b200bfs_handle* h, int index) {
+  return guarded(h, [&](Engine& e) {
+    require(e.prepared && e.bs.allocated && e.bs.K > 0, B200BFS_ERR_STATE, "no batch has run");
+    require(index >= 0 && index < e.bs.K, B200BFS_ERR_INVALID, "index out of range");
+    b200bfs::batch_select(e.g, e.st, e.bs, e.stream, e.sms, index);
+    e.have_run = true;
+    e.last_root = e.bs.roots[(size_t)index];
   });
 }
 

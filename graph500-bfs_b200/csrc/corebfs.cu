@@ -431,33 +431,53 @@ void core_reset_unreachable(DeviceArena& arena, cudaStream_t s, int sms, Graph& 
   rebuild_tree_list(arena, s, sms, g);
 }
 
-void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
-                  int edgefactor, double alpha, double beta, int64_t* at, const RunOptions& opt,
-                  b200bfs_run_stats* stats) {
+void core_climb(const Graph& g, int64_t root, std::vector<int64_t>& path_v,
+                std::vector<int64_t>& path_e, int64_t* entry, int64_t* entry_level) {
   // bfs_tree_with_callback: climb to the 2-core, each vertex taking the
   // previous one as parent at the climbed distance.
-  PathArg path;
-  path.n = 0;
+  path_v.clear();
+  path_e.clear();
   int64_t u = root, p = root, lv = 0;
   const std::vector<int32_t>& tp = g.core.h_tree_parent;
   for (;; ++lv) {
-    if (path.n >= kMaxPath) throw Error{B200BFS_ERR_OVERFLOW, "tree climb longer than 48"};
-    path.v[path.n] = p;
-    path.e[path.n] = pred_entry(u, lv);
-    ++path.n;
+    if ((int)path_v.size() >= kMaxPath) throw Error{B200BFS_ERR_OVERFLOW, "tree climb longer than 48"};
+    path_v.push_back(p);
+    path_e.push_back(pred_entry(u, lv));
     u = p;
     p = tp[u];
     if (p < 0) break;
   }
-  run_bfs_core(g, st, s, sms, u, lv, edgefactor, alpha, beta, at, opt, stats);
+  *entry = u;
+  *entry_level = lv;
+}
+
+int core_write_tree(const Graph& g, int64_t* pred, const std::vector<int64_t>& path_v,
+                    const std::vector<int64_t>& path_e, cudaStream_t s, int sms) {
+  PathArg path;
+  path.n = (int)path_v.size();
+  for (int i = 0; i < path.n; ++i) {
+    path.v[i] = path_v[(size_t)i];
+    path.e[i] = path_e[(size_t)i];
+  }
   const int64_t nt = g.core.tree_vertices;
   if (nt > 0)
-    write_tree_kernel<<<grid_for(nt, 256, sms, 8), 256, 0, s>>>(g.core.tree_list, nt, st.pred);
-  write_path_kernel<<<1, 64, 0, s>>>(path, st.pred);
-  check_cuda(cudaGetLastError(), "core bfs");
+    write_tree_kernel<<<grid_for(nt, 256, sms, 8), 256, 0, s>>>(g.core.tree_list, nt, pred);
+  write_path_kernel<<<1, 64, 0, s>>>(path, pred);
+  check_cuda(cudaGetLastError(), "core tree parents");
+  return (nt > 0 ? 1 : 0) + 1;
+}
+
+void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
+                  int edgefactor, double alpha, double beta, int64_t* at, const RunOptions& opt,
+                  b200bfs_run_stats* stats) {
+  std::vector<int64_t> pv, pe;
+  int64_t u = root, lv = 0;
+  core_climb(g, root, pv, pe, &u, &lv);
+  run_bfs_core(g, st, s, sms, u, lv, edgefactor, alpha, beta, at, opt, stats);
+  const int launches = core_write_tree(g, st.pred, pv, pe, s, sms);
   if (stats) {
-    stats->algorithmic_bytes += 16 * nt;
-    stats->kernel_launches += (nt > 0 ? 1 : 0) + 1;
+    stats->algorithmic_bytes += 16 * g.core.tree_vertices;
+    stats->kernel_launches += launches;
   }
 }
 

@@ -1,0 +1,860 @@
+// Batched multi-source direction-optimizing BFS (up to 64 roots).
+//
+// The reference runs one root per BfsBase::run_bfs call (main.cc:610-640).
+// Here up to 64 roots share one traversal.  State per searched row v:
+//   seen[v]        uint64, bit k set once root k has reached v;
+//   planes[L][v]   uint64, bit k set iff level_k(v) == L (the bit-sliced
+//                  level array of the batch; it is also the frontier of
+//                  level L).
+// Each root keeps its own direction, decided with the reference's switch
+// rule (bfs.hpp:3413-3457) on that root's frontier: roots in top-down mode
+// are expanded by an edge-balanced push over the rows whose plane has one of
+// their bits (batch_td_kernel), roots in bottom-up mode are found by one
+// shared pull sweep (batch_bu_kernel) in which every row with unseen
+// bottom-up bits reads its neighbours' frontier masks, highest-degree
+// neighbours first, until all those bits are found or the row is exhausted.
+// One adjacency read serves every root that needs it.
+//
+// The plan of each level (masks, plane pointers, queue size) lives in a
+// device control block written by batch_control_kernel, so the launch
+// sequence of a level does not depend on host decisions; the host loop only
+// reads back whether to continue.
+#include <algorithm>
+#include <cstring>
+#include "common.cuh"
+#include "corebfs.h"
+#include "msbfs.h"
+
+namespace b200bfs {
+namespace {
+
+constexpr int kQThreads = 256;
+constexpr int kQRows = 8;                        // rows per thread in the queue kernels
+constexpr int kQBlockRows = kQThreads * kQRows;  // rows per block
+constexpr int kBTile = 256;                      // adjacency entries per warp tile (top-down)
+constexpr int64_t kSampleHead = 32768;           // rows always counted in the per-root statistics
+constexpr int kSampleStride = 64;                // then one 32-row chunk in 64
+
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long x) {
+  const unsigned lo = __reduce_or_sync(kFull, (unsigned)x);
+  const unsigned hi = __reduce_or_sync(kFull, (unsigned)(x >> 32));
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long* plane_ptr(const BatchCtl* c, long long L) {
+  return c->planes + L * c->R;
+}
+
+// seen = 0 and planes[0] = 0.
+__global__ void batch_zero_kernel(unsigned long long* __restrict__ a,
+                                  unsigned long long* __restrict__ b, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    a[i] = 0ull;
+    b[i] = 0ull;
+  }
+}
+
+// Queue pass 1 (top-down levels): per-block count and degree sum of the rows
+// whose previous plane holds a top-down root.  Also zero-fills the plane of
+// the level, which the top-down push then ORs into.  Runs when the level has
+// a top-down part or no bottom-up part (the bottom-up sweep otherwise writes
+// every row of the plane itself).
+__global__ void __launch_bounds__(kQThreads) batch_queue_count_kernel(
+    const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
+    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg) {
+  const int has_td = ctl->has_td;
+  if (!has_td && ctl->has_bu) return;
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const unsigned long long T = ctl->td_mask;
+  const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
+  unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
+  const int64_t base = (int64_t)blockIdx.x * kQBlockRows;
+  int64_t cnt = 0, deg = 0;
+#pragma unroll
+  for (int i = 0; i < kQRows; ++i) {
+    const int64_t v = base + i * kQThreads + threadIdx.x;
+    if (v < R) {
+      cur[v] = 0ull;
+      if (has_td && (prev[v] & T)) {
+        ++cnt;
+        deg += row_ptr[v + 1] - row_ptr[v];
+      }
+    }
+  }
+  if (!has_td) return;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    cnt += __shfl_xor_sync(kFull, cnt, o);
+    deg += __shfl_xor_sync(kFull, deg, o);
+  }
+  __shared__ int64_t s_c[kQThreads / 32], s_d[kQThreads / 32];
+  if (lane_id() == 0) {
+    s_c[threadIdx.x >> 5] = cnt;
+    s_d[threadIdx.x >> 5] = deg;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t a = 0, b = 0;
+    for (int i = 0; i < kQThreads / 32; ++i) {
+      a += s_c[i];
+      b += s_d[i];
+    }
+    blk_cnt[blockIdx.x] = a;
+    blk_deg[blockIdx.x] = b;
+  }
+}
+
+__device__ __forceinline__ void warp_scan2(int64_t& a, int64_t& b) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t ta = __shfl_up_sync(kFull, a, o);
+    const int64_t tb = __shfl_up_sync(kFull, b, o);
+    if (lane >= o) {
+      a += ta;
+      b += tb;
+    }
+  }
+}
+
+// Queue pass 2: exclusive scan of the block partials (one block).
+__global__ void __launch_bounds__(1024) batch_queue_scan_kernel(BatchCtl* __restrict__ ctl,
+                                                                int64_t* __restrict__ blk_cnt,
+                                                                int64_t* __restrict__ blk_deg,
+                                                                int64_t nblk,
+                                                                int64_t* __restrict__ qdeg) {
+  if (!ctl->has_td) return;
+  __shared__ int64_t s_a[32], s_b[32];
+  const int t = threadIdx.x;
+  const int64_t per = (nblk + blockDim.x - 1) / blockDim.x;
+  const int64_t lo = min(nblk, t * per), hi = min(nblk, lo + per);
+  int64_t a = 0, b = 0;
+  for (int64_t i = lo; i < hi; ++i) {
+    a += blk_cnt[i];
+    b += blk_deg[i];
+  }
+  int64_t ia = a, ib = b;
+  warp_scan2(ia, ib);
+  const int wid = t >> 5, lane = lane_id();
+  if (lane == 31) {
+    s_a[wid] = ia;
+    s_b[wid] = ib;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    int64_t xa = s_a[lane], xb = s_b[lane];
+    warp_scan2(xa, xb);
+    s_a[lane] = xa;
+    s_b[lane] = xb;
+  }
+  __syncthreads();
+  int64_t ea = ia - a + (wid ? s_a[wid - 1] : 0);
+  int64_t eb = ib - b + (wid ? s_b[wid - 1] : 0);
+  for (int64_t i = lo; i < hi; ++i) {
+    const int64_t ca = blk_cnt[i], cb = blk_deg[i];
+    blk_cnt[i] = ea;
+    blk_deg[i] = eb;
+    ea += ca;
+    eb += cb;
+  }
+  if (t == blockDim.x - 1) {
+    ctl->c.qsize = (unsigned long long)s_a[31];
+    ctl->c.qedges = (unsigned long long)s_b[31];
+    qdeg[s_a[31]] = s_b[31];
+  }
+}
+
+// Queue pass 3: queue rows and their degree prefix.
+__global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
+    const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
+    const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
+    int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
+  if (!ctl->has_td) return;
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const unsigned long long T = ctl->td_mask;
+  const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
+  const int64_t base = (int64_t)blockIdx.x * kQBlockRows;
+  unsigned take = 0;
+  int64_t cnt = 0, deg = 0;
+  int64_t d[kQRows];
+#pragma unroll
+  for (int i = 0; i < kQRows; ++i) {
+    const int64_t v = base + i * kQThreads + threadIdx.x;
+    d[i] = 0;
+    if (v < R && (prev[v] & T)) {
+      take |= 1u << i;
+      d[i] = row_ptr[v + 1] - row_ptr[v];
+      ++cnt;
+      deg += d[i];
+    }
+  }
+  int64_t ic = cnt, id = deg;
+  warp_scan2(ic, id);
+  __shared__ int64_t s_c[kQThreads / 32], s_d[kQThreads / 32];
+  const int wid = threadIdx.x >> 5;
+  if (lane_id() == 31) {
+    s_c[wid] = ic;
+    s_d[wid] = id;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t a = 0, b = 0;
+    for (int i = 0; i < kQThreads / 32; ++i) {
+      const int64_t xa = s_c[i], xb = s_d[i];
+      s_c[i] = a;
+      s_d[i] = b;
+      a += xa;
+      b += xb;
+    }
+  }
+  __syncthreads();
+  int64_t pos = blk_cnt[blockIdx.x] + s_c[wid] + ic - cnt;
+  int64_t dpos = blk_deg[blockIdx.x] + s_d[wid] + id - deg;
+#pragma unroll
+  for (int i = 0; i < kQRows; ++i) {
+    if (take & (1u << i)) {
+      queue[pos] = (int32_t)(base + i * kQThreads + threadIdx.x);
+      qdeg[pos] = dpos;
+      ++pos;
+      dpos += d[i];
+    }
+  }
+}
+
+// Top-down push for the roots in td_mask: edge-balanced over the queue rows
+// (each warp takes kBTile adjacency entries of the concatenated rows).  For
+// an edge (u, v) the bits f = planes[L-1][u] & td_mask not yet in seen[v]
+// are claimed with a fetch-OR on seen[v]; the bits this thread actually
+// claimed go into planes[L][v].  Every (root, vertex) pair is thus claimed
+// exactly once, by a parent at level L-1.
+__global__ void __launch_bounds__(256) batch_td_kernel(
+    BatchCtl* __restrict__ ctl, const int32_t* __restrict__ queue,
+    const int64_t* __restrict__ qdeg, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col) {
+  if (!ctl->has_td) return;
+  const int64_t qsize = (int64_t)ctl->c.qsize;
+  if (qsize == 0) return;
+  const long long L = ctl->level;
+  const unsigned long long T = ctl->td_mask;
+  const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
+  unsigned long long* cur = plane_ptr(ctl, L);
+  unsigned long long* seen = ctl->seen;
+  const int64_t total = qdeg[qsize];
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (total + kBTile - 1) / kBTile;
+  unsigned long long found = 0;
+  for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
+    const int64_t t0 = tile * kBTile;
+    int64_t i0 = 0;
+    if (lane == 0) {
+      int64_t lo = 0, hi = qsize - 1;  // largest i with qdeg[i] <= t0
+      while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (qdeg[mid] <= t0) lo = mid;
+        else hi = mid - 1;
+      }
+      i0 = lo;
+    }
+    int64_t i = __shfl_sync(kFull, i0, 0);
+    int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
+    int32_t src = queue[i];
+    int64_t rbeg = row_ptr[src];
+    unsigned long long f = prev[src] & T;
+#pragma unroll 1
+    for (int k = 0; k < kBTile / 32; ++k) {
+      const int64_t e = t0 + k * 32 + lane;
+      if (e >= total) break;
+      while (e >= seg_hi && i + 1 < qsize) {
+        ++i;
+        seg_lo = seg_hi;
+        seg_hi = qdeg[i + 1];
+        src = queue[i];
+        rbeg = row_ptr[src];
+        f = prev[src] & T;
+      }
+      const int32_t u = __ldg(col + rbeg + (e - seg_lo));
+      // L2 read: seen changes during the kernel; a stale value only costs a
+      // fetch-OR that claims nothing
+      const unsigned long long m = f & ~__ldcg(seen + u);
+      if (m) {
+        const unsigned long long nw = m & ~atomicOr(seen + u, m);
+        if (nw) {
+          atomicOr(cur + u, nw);
+          found |= nw;
+        }
+      }
+    }
+  }
+  found = warp_or64(found);
+  if (lane == 0 && found) atomicOr(&ctl->c.active, found);
+}
+
+// Bottom-up pull for the roots in bu_mask_active.  A warp owns 32
+// consecutive rows (one per lane).  A lane whose row misses some of those
+// roots (U = ~seen & mask) ORs the frontier masks planes[L-1][u] of its
+// neighbours, kProbe of them four loads at a time, until every bit of U is
+// found; rows still open after that are swept by the whole warp, 32
+// neighbours per step, stopping as soon as U is covered.  Rows are sorted by
+// descending degree, so neighbour lists start with the hubs, which most
+// roots reach first.  The row's new bits are written to planes[L] and seen
+// by the lane that owns it: no atomics.  The frontier masks of level L-1 are
+// only read here, and a bit of U can only come from a neighbour at level
+// L-1 of that root, so the OR over neighbours is exact.
+template <int kProbe>
+__global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ctl,
+                                                       const int64_t* __restrict__ row_ptr,
+                                                       const int32_t* __restrict__ col) {
+  if (!ctl->has_bu) return;
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const unsigned long long Bm = ctl->bu_mask_active;
+  const bool has_td = ctl->has_td != 0;
+  const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
+  unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
+  unsigned long long* __restrict__ seen = ctl->seen;
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nchunks = (R + 31) >> 5;
+  unsigned long long found = 0, scanned = 0, rows = 0;
+  for (int64_t ch = gw; ch < nchunks; ch += nwarps) {
+    const int64_t v = ch * 32 + lane;
+    const bool valid = v < R;
+    const unsigned long long s = valid ? seen[v] : ~0ull;
+    const unsigned long long U = ~s & Bm;
+    const unsigned work = __ballot_sync(kFull, U != 0);
+    if (!work) {
+      if (!has_td && valid) cur[v] = 0ull;
+      continue;
+    }
+    rows += (lane == 0) ? __popc(work) : 0;
+    unsigned long long acc = 0;
+    int64_t j = 0, e = 0;
+    if (U) {
+      j = row_ptr[v];
+      e = row_ptr[v + 1];
+    }
+#pragma unroll 1
+    for (int p = 0; p < kProbe; p += 4) {
+      const bool need = (acc & U) != U && j < e;
+      if (!__any_sync(kFull, need)) break;
+      if (need) {
+        const int64_t r = e - j;
+        const int32_t u0 = __ldg(col + j);
+        const int32_t u1 = r > 1 ? __ldg(col + j + 1) : u0;
+        const int32_t u2 = r > 2 ? __ldg(col + j + 2) : u0;
+        const int32_t u3 = r > 3 ? __ldg(col + j + 3) : u0;
+        acc |= __ldg(prev + u0) | __ldg(prev + u1) | __ldg(prev + u2) | __ldg(prev + u3);
+        const int64_t t = r < 4 ? r : 4;
+        j += t;
+        scanned += t;
+      }
+    }
+    unsigned rem = __ballot_sync(kFull, (acc & U) != U && j < e);
+    while (rem) {
+      const int l = __ffs(rem) - 1;
+      rem &= rem - 1;
+      const int64_t jb = __shfl_sync(kFull, j, l), je = __shfl_sync(kFull, e, l);
+      const unsigned long long Ul = __shfl_sync(kFull, U, l);
+      unsigned long long al = __shfl_sync(kFull, acc, l);
+      int64_t jj = jb;
+      while (jj < je) {
+        const int64_t x = jj + lane;
+        unsigned long long m = 0;
+        if (x < je) m = __ldg(prev + __ldg(col + x));
+        al |= warp_or64(m);
+        jj += 32;
+        if ((al & Ul) == Ul) break;
+      }
+      if (lane == l) {
+        acc = al;
+        scanned += (unsigned long long)(min(jj, je) - jb);
+      }
+    }
+    const unsigned long long n = acc & U;
+    if (valid) {
+      if (!has_td) cur[v] = n;
+      else if (n) cur[v] |= n;
+      if (n) seen[v] = s | n;
+    }
+    found |= n;
+  }
+  found = warp_or64(found);
+  scanned = warp_sum64(scanned);
+  if (lane == 0) {
+    if (found) atomicOr(&ctl->c.active, found);
+    if (scanned) atomicAdd(&ctl->c.scanned_bu, scanned);
+    if (rows) atomicAdd(&ctl->c.rows_bu, rows);
+  }
+}
+
+// Per-root frontier size and pre-dedup degree sum of level L, the inputs of
+// the switch rule.  They only steer the direction (levels do not depend on
+// them), so they are estimated: the first kSampleHead rows (the hubs, which
+// carry most of the degree mass) are counted exactly, the rest through one
+// 32-row chunk in kSampleStride, weighted by kSampleStride.
+__global__ void __launch_bounds__(256) batch_stats_kernel(BatchCtl* __restrict__ ctl,
+                                                          const int32_t* __restrict__ mdeg) {
+  __shared__ unsigned long long s_cnt[kBatchMax], s_edg[kBatchMax];
+  if (threadIdx.x < kBatchMax) {
+    s_cnt[threadIdx.x] = 0;
+    s_edg[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
+  const int64_t head = R < kSampleHead ? R : kSampleHead;
+  const int64_t head_w = (head + 31) >> 5;
+  const int64_t tail_w =
+      R > head ? (R - head + 32 * kSampleStride - 1) / (32 * kSampleStride) : 0;
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t w = gw; w < head_w + tail_w; w += nwarps) {
+    int64_t v;
+    unsigned long long wt;
+    if (w < head_w) {
+      v = w * 32 + lane;
+      wt = 1;
+    } else {
+      v = head + (w - head_w) * 32 * kSampleStride + lane;
+      wt = kSampleStride;
+    }
+    const unsigned long long n = v < R ? cur[v] : 0ull;
+    unsigned long long any = warp_or64(n);
+    if (!any) continue;
+    const unsigned d = v < R ? (unsigned)min(mdeg[v], 1 << 26) : 0u;
+    while (any) {
+      const int k = __ffsll((long long)any) - 1;
+      any &= any - 1;
+      const bool b = (n >> k) & 1ull;
+      const unsigned c = __popc(__ballot_sync(kFull, b));
+      const unsigned ds = __reduce_add_sync(kFull, b ? d : 0u);
+      if (lane == 0) {
+        atomicAdd(&s_cnt[k], (unsigned long long)c * wt);
+        atomicAdd(&s_edg[k], (unsigned long long)ds * wt);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kBatchMax && s_cnt[threadIdx.x]) {
+    atomicAdd(&ctl->c.cnt[threadIdx.x], s_cnt[threadIdx.x]);
+    atomicAdd(&ctl->c.edg[threadIdx.x], s_edg[threadIdx.x]);
+  }
+}
+
+// Closes level L = ctl->level and plans level L + 1 (one thread).
+//  - roots whose entry level is L (L = 0, or the CoreBFS climb length) are
+//    seeded into planes[L] and seen;
+//  - the level is recorded;
+//  - each root with a frontier applies the reference's switch rule to its
+//    own frontier (bfs.hpp:3413-3457): top-down -> bottom-up when its
+//    frontier grew and its edge count exceeds num_global_edges / alpha,
+//    bottom-up -> top-down when it shrank below
+//    num_global_verts / (beta * edgefactor * 2); a root seeded in this
+//    level is not tested, as the reference does not test level 0;
+//  - done = 1 when no root has a frontier and none is still to enter,
+//    2 when planes[L + 1] is not allocated, 3 past level 0xFFFE.
+// With a graph conditional handle it also sets the loop condition.
+__global__ void batch_control_kernel(BatchCtl* __restrict__ ctl, const int32_t* __restrict__ mdeg,
+                                     cudaGraphConditionalHandle cond, int use_cond) {
+  BatchCtl& c = *ctl;
+  const long long L = c.level;
+  unsigned long long* cur = plane_ptr(ctl, L);
+  unsigned long long seeded = 0;
+  unsigned long long pend = c.pending;
+  while (pend) {
+    const int k = __ffsll((long long)pend) - 1;
+    pend &= pend - 1;
+    if (c.root_lv[k] != L) continue;
+    const unsigned long long bit = 1ull << k;
+    c.pending &= ~bit;
+    const int r = c.root_row[k];
+    if (r < 0) continue;
+    cur[r] |= bit;
+    c.seen[r] |= bit;
+    c.c.active |= bit;
+    seeded |= bit;
+  }
+  if (L < kBatchHist) {
+    BatchLevelRec& h = c.hist[L];
+    h.td_roots = c.has_td ? c.td_mask : 0ull;
+    h.bu_roots = c.has_bu ? c.bu_mask_active : 0ull;
+    h.active = c.c.active;
+    h.scanned_bu = c.c.scanned_bu;
+    h.rows_bu = c.c.rows_bu;
+    h.qsize = c.has_td ? c.c.qsize : 0ull;
+    h.qedges = c.has_td ? c.c.qedges : 0ull;
+  }
+  const unsigned long long act = c.c.active;
+  const long long e_thr = (long long)(c.nedges / c.alpha);
+  const long long n_thr = (long long)(c.nverts / (c.beta * c.edgefactor * 2.0));
+  unsigned long long it = act & ~seeded;
+  while (it) {
+    const int k = __ffsll((long long)it) - 1;
+    it &= it - 1;
+    const unsigned long long bit = 1ull << k;
+    const long long n = (long long)c.c.cnt[k], e = (long long)c.c.edg[k];
+    if ((c.growing & bit) && n > c.prev_cnt[k]) {
+      if (!(c.bu_mask & bit) && e > e_thr) c.bu_mask |= bit;
+    } else if (c.bu_mask & bit) {
+      if (n < n_thr) {
+        c.bu_mask &= ~bit;
+        c.growing &= ~bit;
+      }
+    }
+    c.prev_cnt[k] = n;
+  }
+  unsigned long long sd = seeded;
+  while (sd) {
+    const int k = __ffsll((long long)sd) - 1;
+    sd &= sd - 1;
+    c.prev_cnt[k] = 0;
+  }
+  int done = 0;
+  if (act == 0 && c.pending == 0) {
+    done = 1;
+  } else if (L + 1 > kMaxLevel) {
+    done = 3;
+  } else {
+    c.level = L + 1;
+    c.td_mask = act & ~c.bu_mask;
+    c.bu_mask_active = act & c.bu_mask;
+    c.has_td = c.td_mask != 0;
+    c.has_bu = c.bu_mask_active != 0;
+    memset(&c.c, 0, sizeof(BatchCounters));
+    if (L + 1 >= c.capacity) done = 2;
+  }
+  c.done = done;
+  if (use_cond) cudaGraphSetConditional(cond, done == 0 ? 1u : 0u);
+}
+
+struct BatchSetupArg {
+  unsigned long long* planes;
+  unsigned long long* seen;
+  long long R, capacity, nedges, nverts;
+  double alpha, beta;
+  int edgefactor, K;
+  long long v[kBatchMax];  // entry vertex of each root (original id)
+  int lv[kBatchMax];       // its level
+};
+
+// Initialises the control block for a new batch (64 threads).
+__global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, BatchSetupArg a,
+                                   const int32_t* __restrict__ rank, int64_t nverts) {
+  const int t = threadIdx.x;
+  if (t < kBatchMax) {
+    const bool ok = t < a.K && a.v[t] >= 0 && a.v[t] < nverts;
+    ctl->root_row[t] = ok ? rank[a.v[t]] : -1;
+    ctl->root_lv[t] = t < a.K ? a.lv[t] : 0;
+    ctl->prev_cnt[t] = 0;
+  }
+  if (t == 0) {
+    ctl->planes = a.planes;
+    ctl->seen = a.seen;
+    ctl->R = a.R;
+    ctl->capacity = a.capacity;
+    ctl->nedges = a.nedges;
+    ctl->nverts = a.nverts;
+    ctl->alpha = a.alpha;
+    ctl->beta = a.beta;
+    ctl->edgefactor = a.edgefactor;
+    ctl->K = a.K;
+    const unsigned long long all = a.K >= 64 ? ~0ull : ((1ull << a.K) - 1);
+    ctl->level = 0;
+    ctl->td_mask = 0;
+    ctl->bu_mask_active = 0;
+    ctl->has_td = 0;
+    ctl->has_bu = 0;
+    ctl->done = 0;
+    ctl->bu_mask = 0;
+    ctl->growing = all;
+    ctl->pending = all;
+    memset(&ctl->c, 0, sizeof(BatchCounters));
+  }
+}
+
+// Points the control block at a larger plane pool and resumes the search.
+__global__ void batch_pool_kernel(BatchCtl* ctl, unsigned long long* planes, long long capacity) {
+  ctl->planes = planes;
+  ctl->capacity = capacity;
+  ctl->done = 0;
+}
+
+// Level of root k for every row (-1: not reached), from the planes.
+__global__ void batch_row_levels_kernel(const unsigned long long* __restrict__ planes, int64_t R,
+                                        int64_t nplanes, int k, int32_t* __restrict__ out) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < R;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    int32_t lv = -1;
+    for (int64_t L = 0; L < nplanes; ++L)
+      if ((planes[L * R + v] >> k) & 1ull) {
+        lv = (int32_t)L;
+        break;
+      }
+    out[v] = lv;
+  }
+}
+
+__global__ void fill_minus_one_kernel(int64_t* __restrict__ p, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = -1;
+}
+
+// pred of one root from its row levels: the entry row is its own parent,
+// every other reached row takes its first neighbour one level nearer.
+__global__ void batch_parent_kernel(const int32_t* __restrict__ lv, int64_t R,
+                                    const int64_t* __restrict__ row_ptr,
+                                    const int32_t* __restrict__ col,
+                                    const int32_t* __restrict__ inv, int root_row,
+                                    int64_t* __restrict__ pred, int* __restrict__ missing) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < R;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t L = lv[v];
+    if (L < 0) continue;
+    const int64_t me = inv[v];
+    if (v == root_row) {
+      pred[me] = pred_entry(me, L);
+      continue;
+    }
+    bool found = false;
+    for (int64_t j = row_ptr[v], e = row_ptr[v + 1]; j < e; ++j) {
+      const int32_t u = col[j];
+      if (lv[u] == L - 1) {
+        pred[me] = pred_entry(inv[u], L);
+        found = true;
+        break;
+      }
+    }
+    if (!found) atomicExch(missing, 1);
+  }
+}
+
+__global__ void set_entry_kernel(int64_t* p, int64_t i, int64_t value) { p[i] = value; }
+
+}  // namespace
+
+cudaEvent_t BatchState::event(size_t i) {
+  while (ev.size() <= i) {
+    cudaEvent_t e;
+    check_cuda(cudaEventCreate(&e), "event");
+    ev.push_back(e);
+  }
+  return ev[i];
+}
+
+void BatchState::release(DeviceArena& arena) {
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  ev.clear();
+  if (!allocated) return;
+  arena.free(planes);
+  arena.free(seen);
+  arena.free(blk_cnt);
+  arena.free(blk_deg);
+  arena.free(ctl);
+  cudaFreeHost(hctl);
+  cudaFreeHost(hdone);
+  planes = seen = nullptr;
+  blk_cnt = blk_deg = nullptr;
+  ctl = nullptr;
+  hctl = nullptr;
+  hdone = nullptr;
+  capacity = 0;
+  allocated = false;
+  K = 0;
+  levels = 0;
+}
+
+namespace {
+
+void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
+  bs.release(arena);
+  bs.R = g.csr.nrows;
+  bs.nblk = (bs.R + kQBlockRows - 1) / kQBlockRows;
+  bs.seen = arena_alloc<unsigned long long>(arena, bs.R, "batch seen masks");
+  bs.blk_cnt = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block counts");
+  bs.blk_deg = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block degrees");
+  bs.ctl = arena_alloc<BatchCtl>(arena, 1, "batch control block");
+  check_cuda(cudaMallocHost(&bs.hctl, sizeof(BatchCtl)), "pinned batch control");
+  check_cuda(cudaMallocHost(&bs.hdone, sizeof(int)), "pinned flag");
+  bs.allocated = true;
+  // Level planes: 16 to start with (Kronecker searches need about 10),
+  // fewer when memory is short; the search grows the pool when it runs out.
+  for (int64_t cap = 16;; cap /= 2) {
+    try {
+      bs.planes = arena_alloc<unsigned long long>(arena, cap * bs.R, "batch level planes");
+      bs.capacity = cap;
+      break;
+    } catch (const Error& e) {
+      if (e.code != B200BFS_ERR_OOM || cap <= 2) throw;
+    }
+  }
+}
+
+// Doubles the plane pool, keeping planes [0, used).
+void batch_grow(DeviceArena& arena, BatchState& bs, int64_t used, cudaStream_t s) {
+  const int64_t cap = bs.capacity * 2;
+  unsigned long long* np = arena_alloc<unsigned long long>(arena, cap * bs.R, "batch level planes");
+  check_cuda(cudaMemcpyAsync(np, bs.planes, (size_t)used * bs.R * 8, cudaMemcpyDeviceToDevice, s),
+             "copy planes");
+  batch_pool_kernel<<<1, 1, 0, s>>>(bs.ctl, np, cap);
+  check_cuda(cudaStreamSynchronize(s), "grow planes");
+  arena.free(bs.planes);
+  bs.planes = np;
+  bs.capacity = cap;
+}
+
+}  // namespace
+
+void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
+               int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
+               b200bfs_batch_stats* stats) {
+  const Csr& c = g.csr;
+  if (!bs.allocated || bs.R != c.nrows) batch_allocate(arena, g, bs);
+  BatchSetupArg a;
+  memset(&a, 0, sizeof(a));
+  bs.roots.assign(roots, roots + k);
+  bs.entry_vertex.assign((size_t)k, -1);
+  bs.entry_level.assign((size_t)k, 0);
+  bs.path_v.assign((size_t)k, {});
+  bs.path_e.assign((size_t)k, {});
+  for (int i = 0; i < k; ++i) {
+    int64_t entry = roots[i], lv = 0;
+    if (g.core.enabled) core_climb(g, roots[i], bs.path_v[i], bs.path_e[i], &entry, &lv);
+    bs.entry_vertex[i] = entry;
+    bs.entry_level[i] = (int32_t)lv;
+    a.v[i] = entry;
+    a.lv[i] = (int)lv;
+  }
+  a.planes = bs.planes;
+  a.seen = bs.seen;
+  a.R = bs.R;
+  a.capacity = bs.capacity;
+  a.nedges = c.nedges;
+  a.nverts = c.nrows;
+  a.alpha = alpha > 0 ? alpha : kBatchAlpha;
+  a.beta = beta;
+  a.edgefactor = edgefactor;
+  a.K = k;
+  bs.K = k;
+
+  const int B = 256;
+  size_t nev = 0;
+  check_cuda(cudaEventRecord(bs.event(nev++), s), "event");
+  batch_zero_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.seen, bs.planes, bs.R);
+  batch_setup_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, a, c.rank, g.nverts);
+  batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
+  int launches = 3;
+  const unsigned nblk = (unsigned)std::max<int64_t>(bs.nblk, 1);
+  std::vector<std::pair<size_t, size_t>> bu_ev;
+  for (;;) {
+    batch_queue_count_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg);
+    batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, st.qdeg);
+    batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt,
+                                                        bs.blk_deg, st.queue, st.qdeg);
+    batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, st.queue, st.qdeg, c.row_ptr, c.col);
+    check_cuda(cudaEventRecord(bs.event(nev), s), "event");
+    batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col);
+    check_cuda(cudaEventRecord(bs.event(nev + 1), s), "event");
+    bu_ev.push_back({nev, nev + 1});
+    nev += 2;
+    batch_stats_kernel<<<sms * 2, B, 0, s>>>(bs.ctl, c.mdeg);
+    batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
+    launches += 7;
+    check_cuda(cudaMemcpyAsync(bs.hdone, &bs.ctl->done, sizeof(int), cudaMemcpyDeviceToHost, s),
+               "batch flag");
+    check_cuda(cudaStreamSynchronize(s), "batch level");
+    const int done = *bs.hdone;
+    if (done == 0) continue;
+    if (done == 1) break;
+    if (done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
+    // done == 2: the next level needs another plane
+    check_cuda(cudaMemcpyAsync(bs.hctl, bs.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s),
+               "batch control");
+    check_cuda(cudaStreamSynchronize(s), "batch control");
+    batch_grow(arena, bs, bs.hctl->level, s);
+    ++launches;
+  }
+  check_cuda(cudaEventRecord(bs.event(nev++), s), "event");
+  check_cuda(cudaMemcpyAsync(bs.hctl, bs.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s),
+             "batch control");
+  check_cuda(cudaStreamSynchronize(s), "batch");
+  check_cuda(cudaGetLastError(), "batch");
+  const BatchCtl& h = *bs.hctl;
+  // the last level found nothing: planes [0, level) hold the levels
+  bs.levels = h.level;
+  if (stats) {
+    b200bfs_batch_stats r;
+    memset(&r, 0, sizeof(r));
+    r.num_roots = k;
+    r.levels = (int32_t)std::max<long long>(h.level - 1, 0);
+    r.kernel_launches = launches;
+    const int64_t R = bs.R;
+    int64_t bytes = 16 * R;  // seen and plane 0
+    for (long long L = 1; L <= h.level && L < kBatchHist; ++L) {
+      const BatchLevelRec& x = h.hist[L];
+      if (x.td_roots) {
+        ++r.num_td_levels;
+        r.edges_scanned_td += (int64_t)x.qedges;
+        bytes += 16 * (int64_t)x.qsize + 12 * (int64_t)x.qedges;
+      }
+      if (x.bu_roots) {
+        ++r.num_bu_levels;
+        r.edges_scanned_bu += (int64_t)x.scanned_bu;
+        const int64_t b = 16 * R + 16 * (int64_t)x.rows_bu + 12 * (int64_t)x.scanned_bu;
+        r.bu_bytes += b;
+        bytes += b;
+      } else {
+        bytes += 8 * R;  // the level's plane
+      }
+    }
+    r.algorithmic_bytes = bytes;
+    float ms = 0;
+    check_cuda(cudaEventElapsedTime(&ms, bs.ev[0], bs.ev[nev - 1]), "elapsed");
+    r.ms = ms;
+    for (const auto& p : bu_ev) {
+      check_cuda(cudaEventElapsedTime(&ms, bs.ev[p.first], bs.ev[p.second]), "elapsed");
+      r.bu_ms += ms;
+    }
+    *stats = r;
+  }
+}
+
+void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream_t s, int sms,
+                  int index) {
+  const Csr& c = g.csr;
+  const int B = 256;
+  int32_t* lv = st.queue;  // scratch of R + 1 entries
+  batch_row_levels_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.planes, bs.R, bs.levels,
+                                                                 index, lv);
+  fill_minus_one_kernel<<<grid_for(st.pred_size, B, sms, 8), B, 0, s>>>(st.pred, st.pred_size);
+  int* missing = reinterpret_cast<int*>(st.blk_cnt);  // scratch flag
+  check_cuda(cudaMemsetAsync(missing, 0, sizeof(int), s), "memset");
+  const int root_row = bs.hctl->root_row[index];
+  batch_parent_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(lv, bs.R, c.row_ptr, c.col, c.inv,
+                                                              root_row, st.pred, missing);
+  const int64_t root = bs.roots[(size_t)index];
+  if (g.core.enabled)
+    core_write_tree(g, st.pred, bs.path_v[(size_t)index], bs.path_e[(size_t)index], s, sms);
+  else if (root_row < 0 && root >= 0 && root < st.pred_size)
+    set_entry_kernel<<<1, 1, 0, s>>>(st.pred, root, pred_entry(root, 0));
+  int hmissing = 0;
+  check_cuda(cudaMemcpyAsync(&hmissing, missing, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "batch select");
+  if (hmissing) throw Error{B200BFS_ERR_CUDA, "batch levels without a parent one level up"};
+}
+
+}  // namespace b200bfs

@@ -1,0 +1,101 @@
+// Batched multi-source BFS: up to 64 roots traversed together.
+#pragma once
+
+#include "bfs_internal.h"
+
+namespace b200bfs {
+
+constexpr int kBatchMax = 64;        // roots per batch (one bit each of a uint64 mask)
+constexpr int kBatchHist = 256;      // per-level records kept on the device
+constexpr double kBatchAlpha = 30.0; // default top-down -> bottom-up threshold of a batch
+
+// Counters of the level being computed (device).
+struct BatchCounters {
+  unsigned long long active;      // OR of the root bits found in the level (exact)
+  unsigned long long scanned_bu;  // adjacency entries read bottom-up
+  unsigned long long rows_bu;     // rows with unseen bottom-up bits
+  unsigned long long qsize;       // rows of the top-down queue
+  unsigned long long qedges;      // adjacency entries of the top-down queue rows
+  unsigned long long cnt[kBatchMax];  // per-root frontier rows (sampled estimate)
+  unsigned long long edg[kBatchMax];  // per-root pre-dedup degree sum (sampled estimate)
+};
+
+struct BatchLevelRec {
+  unsigned long long td_roots;    // roots expanded top-down in the level
+  unsigned long long bu_roots;    // roots searched bottom-up in the level
+  unsigned long long active;      // roots that found a vertex in the level
+  unsigned long long scanned_bu;
+  unsigned long long rows_bu;
+  unsigned long long qsize;
+  unsigned long long qedges;
+};
+
+// Control block of a batched search, resident on the device.  The level
+// kernels read their plan (level, masks, plane pointers) from it, and the
+// control kernel writes the next plan, so the same launch sequence serves
+// a host-driven loop and a device-side loop in a CUDA graph.
+struct BatchCtl {
+  // fixed during a search
+  unsigned long long* planes;  // [capacity][R]: bit k of planes[L][v] <=> level_k(v) == L
+  unsigned long long* seen;    // [R]: bits of the roots that reached v
+  long long R;
+  long long capacity;          // planes allocated
+  long long nedges;            // num_global_edges (alpha test)
+  long long nverts;            // num_global_verts (beta test)
+  double alpha, beta;
+  int edgefactor;
+  int K;
+  int root_row[kBatchMax];     // row where root k enters the searched graph, -1: none
+  int root_lv[kBatchMax];      // level at which it enters (CoreBFS climb), 0 otherwise
+  // plan of the level being computed
+  long long level;
+  unsigned long long td_mask;  // roots expanded top-down
+  unsigned long long bu_mask_active;  // roots searched bottom-up (with a frontier)
+  int has_td, has_bu;
+  int done;                    // 0 running, 1 finished, 2 needs more planes, 3 level overflow
+  int pad;
+  // per-root switch state (the reference rule, bfs.hpp:3413-3457, per root)
+  unsigned long long bu_mask, growing, pending;
+  long long prev_cnt[kBatchMax];
+  BatchCounters c;
+  BatchLevelRec hist[kBatchHist];
+};
+
+struct BatchState {
+  bool allocated = false;
+  int64_t R = 0;
+  int64_t capacity = 0;
+  int64_t nblk = 0;
+  unsigned long long* planes = nullptr;
+  unsigned long long* seen = nullptr;
+  int64_t* blk_cnt = nullptr;
+  int64_t* blk_deg = nullptr;
+  BatchCtl* ctl = nullptr;   // device
+  BatchCtl* hctl = nullptr;  // pinned mirror
+  int* hdone = nullptr;      // pinned copy of ctl->done
+  std::vector<cudaEvent_t> ev;
+  // last batch
+  int K = 0;
+  int64_t levels = 0;                 // planes in use = last level + 1
+  std::vector<int64_t> roots;         // original ids
+  std::vector<int64_t> entry_vertex;  // vertex where each root enters the searched graph
+  std::vector<int32_t> entry_level;   // level of that vertex (CoreBFS climb length)
+  std::vector<std::vector<int64_t>> path_v, path_e;  // CoreBFS climb of each root
+  cudaEvent_t event(size_t i);
+  void release(DeviceArena& arena);
+};
+
+// Runs one batched search from roots[0..k) over g.csr.  alpha <= 0 selects
+// kBatchAlpha.  The CoreBFS climb of each root is applied as in
+// BfsBase::run_bfs (bfs.hpp:3214-3232).
+void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
+               int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
+               b200bfs_batch_stats* stats);
+
+// Writes root `index` of the last batch into st.pred in the reference
+// encoding: level from the planes, parent = a neighbour one level closer to
+// the root (any such neighbour is a valid BFS parent).
+void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream_t s, int sms,
+                  int index);
+
+}  // namespace b200bfs

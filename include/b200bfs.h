@@ -116,6 +116,22 @@ typedef struct b200bfs_level_stats {
   double ms;                     /* CUDA-event time of the level's kernel    */
 } b200bfs_level_stats;
 
+/* Statistics of the last batched search (b200bfs_run_batch). */
+typedef struct b200bfs_batch_stats {
+  int32_t num_roots;             /* roots in the batch                        */
+  int32_t levels;                /* last level of the deepest root            */
+  int32_t num_td_levels;         /* levels with a top-down expansion          */
+  int32_t num_bu_levels;         /* levels with a bottom-up sweep             */
+  int32_t kernel_launches;
+  int32_t reserved;
+  int64_t edges_scanned_td;      /* adjacency entries read top-down           */
+  int64_t edges_scanned_bu;      /* adjacency entries read bottom-up          */
+  int64_t algorithmic_bytes;     /* bytes the batch must move (roofline)      */
+  int64_t bu_bytes;              /* of which in the bottom-up kernel          */
+  double ms;                     /* CUDA-event time of the whole batch        */
+  double bu_ms;                  /* CUDA-event time of the bottom-up kernels  */
+} b200bfs_batch_stats;
+
 /* --------------------------- lifetime / errors --------------------------- */
 
 /* Replaces `new BfsOnCPU()` (main.cc:433). */
@@ -244,6 +260,30 @@ int b200bfs_end(b200bfs_handle* h);
  * numerator) in *edge_visit_count. */
 int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors,
                      int64_t* edge_visit_count);
+
+/* ---------------------------- batched search ------------------------------ */
+
+#define B200BFS_BATCH_MAX 64
+
+/* No single counterpart in the reference, which runs one root per run_bfs
+ * call (main.cc:610-640); this is that loop over roots done in one
+ * traversal.  Searches from roots[0..num_roots), 1 <= num_roots <= 64, in
+ * one multi-source traversal: every vertex carries a 64-bit mask of the roots
+ * that reached it, so one read of an adjacency row serves all roots.  Each
+ * root switches between top-down and bottom-up on its own, with the rule of
+ * bfs.hpp:3413-3457 applied to that root's frontier (alpha <= 0 selects the
+ * batch default 30; beta as for b200bfs_run).  Per-root levels equal those
+ * of b200bfs_run from the same root.  Requires b200bfs_prepare; with CoreBFS
+ * each root climbs to the 2-core first, as b200bfs_run does.  stats may be
+ * NULL. */
+int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, int edgefactor,
+                      double alpha, double beta, b200bfs_batch_stats* stats);
+
+/* Makes root `index` of the last batch the engine's current result: pred is
+ * rebuilt on the device from the batch's levels (parent = a neighbour one
+ * level nearer the root, a valid BFS parent), so b200bfs_get_pred,
+ * b200bfs_get_levels and b200bfs_validate then report that root. */
+int b200bfs_batch_select(b200bfs_handle* h, int index);
 
 /* ------------------------- allocation-free search ------------------------ */
 
