@@ -91,7 +91,8 @@ class BatchStats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("edges_scanned_td", ctypes.c_int64), ("edges_scanned_bu", ctypes.c_int64),
                 ("algorithmic_bytes", ctypes.c_int64), ("bu_bytes", ctypes.c_int64),
-                ("ms", ctypes.c_double), ("bu_ms", ctypes.c_double)]
+                ("ms", ctypes.c_double), ("bu_ms", ctypes.c_double),
+                ("td_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

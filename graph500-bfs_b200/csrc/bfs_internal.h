@@ -45,6 +45,8 @@ struct RunOptions {
   int td_kernel = 1;        // 1: td_expand_kernel, 2: td_wide_kernel
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
+  int batch_graph = 1;      // batched search: level loop in a CUDA graph (0: host loop)
+  double batch_alpha = 30;  // batched search: alpha used when the caller passes alpha <= 0
 };
 
 void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,

@@ -578,6 +578,12 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "bu_probe") {
       require(value >= 1 && value <= 64, B200BFS_ERR_INVALID, "bu_probe must be 1..64");
       e.opt.bu_probe = (int)value;
+    } else if (n == "batch_graph") {
+      require(value == 0 || value == 1, B200BFS_ERR_INVALID, "batch_graph must be 0 or 1");
+      e.opt.batch_graph = (int)value;
+    } else if (n == "batch_alpha") {
+      require(value >= 1 && value <= 1000000, B200BFS_ERR_INVALID, "batch_alpha must be 1..1e6");
+      e.opt.batch_alpha = (double)value;
     } else if (n == "force_direction") {
       require(value >= 0 && value <= 2, B200BFS_ERR_INVALID, "force_direction must be 0..2");
       e.opt.force_direction = (int)value;
@@ -597,7 +603,7 @@ int b200bfs_get_stream(b200bfs_handle* h, void** stream) {
 int b200bfs_get_level_stats(b200bfs_handle* h, b200bfs_level_stats* out, int max, int* count) {
   return guarded(h, [&](Engine& e) {
     require(count != nullptr && (out != nullptr || max == 0), B200BFS_ERR_INVALID, "null output");
-    require(e.have_run, B200BFS_ERR_STATE, "no search has run");
+    require(e.prepared && !e.st.levels.empty(), B200BFS_ERR_STATE, "no search has run");
     *count = (int)e.st.levels.size();
     for (int i = 0; i < max && i < *count; ++i) out[i] = e.st.levels[(size_t)i];
   });
@@ -631,7 +637,7 @@ int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, in
       require(roots[i] >= 0 && roots[i] < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
     b200bfs_batch_stats rs;
     b200bfs::run_batch(e.arena, e.g, e.st, e.bs, e.stream, e.sms, roots, num_roots, edgefactor,
-                       alpha, beta, &rs);
+                       alpha > 0 ? alpha : e.opt.batch_alpha, beta, e.opt.batch_graph != 0, &rs);
     if (stats) *stats = rs;
     e.have_run = false;
   });

@@ -29,8 +29,6 @@ namespace b200bfs {
 namespace {
 
 constexpr int kQThreads = 256;
-constexpr int kQRows = 8;                        // rows per thread in the queue kernels
-constexpr int kQBlockRows = kQThreads * kQRows;  // rows per block
 constexpr int kBTile = 256;                      // adjacency entries per warp tile (top-down)
 constexpr int64_t kSampleHead = 32768;           // rows always counted in the per-root statistics
 constexpr int kSampleStride = 64;                // then one 32-row chunk in 64
@@ -51,45 +49,48 @@ __device__ __forceinline__ unsigned long long* plane_ptr(const BatchCtl* c, long
   return c->planes + L * c->R;
 }
 
-// seen = 0 and planes[0] = 0.
-__global__ void batch_zero_kernel(unsigned long long* __restrict__ a,
-                                  unsigned long long* __restrict__ b, int64_t n) {
+// Level start: clears the touched-row bitmap of the level and, when no
+// bottom-up sweep will write every row of the level's plane, zero-fills the
+// plane for the top-down push to OR into.
+__global__ void batch_clear_kernel(const BatchCtl* __restrict__ ctl) {
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const int64_t W = (R + 31) >> 5;
+  uint32_t* __restrict__ rb = ctl->rowbits[L & 1];
+  unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
+  const bool zero_plane = !ctl->has_bu;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    a[i] = 0ull;
-    b[i] = 0ull;
-  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < W; i += stride) rb[i] = 0u;
+  if (zero_plane)
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < R; i += stride)
+      cur[i] = 0ull;
 }
 
 // Queue pass 1 (top-down levels): per-block count and degree sum of the rows
-// whose previous plane holds a top-down root.  Also zero-fills the plane of
-// the level, which the top-down push then ORs into.  Runs when the level has
-// a top-down part or no bottom-up part (the bottom-up sweep otherwise writes
-// every row of the plane itself).
+// whose previous plane holds a top-down root.  Only rows marked in the
+// previous level's touched-row bitmap can, so the pass reads that bitmap
+// (one bit per row) and the plane entries of its set bits.  One thread per
+// bitmap word.
 __global__ void __launch_bounds__(kQThreads) batch_queue_count_kernel(
     const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
     int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg) {
-  const int has_td = ctl->has_td;
-  if (!has_td && ctl->has_bu) return;
+  if (!ctl->has_td) return;
   const long long L = ctl->level;
-  const int64_t R = ctl->R;
+  const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
-  unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
-  const int64_t base = (int64_t)blockIdx.x * kQBlockRows;
+  const uint32_t* __restrict__ rb = ctl->rowbits[(L - 1) & 1];
+  const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
   int64_t cnt = 0, deg = 0;
-#pragma unroll
-  for (int i = 0; i < kQRows; ++i) {
-    const int64_t v = base + i * kQThreads + threadIdx.x;
-    if (v < R) {
-      cur[v] = 0ull;
-      if (has_td && (prev[v] & T)) {
-        ++cnt;
-        deg += row_ptr[v + 1] - row_ptr[v];
-      }
+  uint32_t bits = w < W ? rb[w] : 0u;
+  while (bits) {
+    const int64_t v = w * 32 + __ffs(bits) - 1;
+    bits &= bits - 1;
+    if (prev[v] & T) {
+      ++cnt;
+      deg += row_ptr[v + 1] - row_ptr[v];
     }
   }
-  if (!has_td) return;
 #pragma unroll
   for (int o = 16; o; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -172,29 +173,31 @@ __global__ void __launch_bounds__(1024) batch_queue_scan_kernel(BatchCtl* __rest
   }
 }
 
-// Queue pass 3: queue rows and their degree prefix.
+// Queue pass 3: queue rows (in row order) and their degree prefix.
 __global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
     const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
     int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
   if (!ctl->has_td) return;
   const long long L = ctl->level;
-  const int64_t R = ctl->R;
+  const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
-  const int64_t base = (int64_t)blockIdx.x * kQBlockRows;
-  unsigned take = 0;
+  const uint32_t* __restrict__ rb = ctl->rowbits[(L - 1) & 1];
+  const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
+  uint32_t take = 0;
   int64_t cnt = 0, deg = 0;
-  int64_t d[kQRows];
-#pragma unroll
-  for (int i = 0; i < kQRows; ++i) {
-    const int64_t v = base + i * kQThreads + threadIdx.x;
-    d[i] = 0;
-    if (v < R && (prev[v] & T)) {
-      take |= 1u << i;
-      d[i] = row_ptr[v + 1] - row_ptr[v];
-      ++cnt;
-      deg += d[i];
+  {
+    uint32_t bits = w < W ? rb[w] : 0u;
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const int64_t v = w * 32 + b;
+      if (prev[v] & T) {
+        take |= 1u << b;
+        ++cnt;
+        deg += row_ptr[v + 1] - row_ptr[v];
+      }
     }
   }
   int64_t ic = cnt, id = deg;
@@ -219,23 +222,25 @@ __global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
   __syncthreads();
   int64_t pos = blk_cnt[blockIdx.x] + s_c[wid] + ic - cnt;
   int64_t dpos = blk_deg[blockIdx.x] + s_d[wid] + id - deg;
-#pragma unroll
-  for (int i = 0; i < kQRows; ++i) {
-    if (take & (1u << i)) {
-      queue[pos] = (int32_t)(base + i * kQThreads + threadIdx.x);
-      qdeg[pos] = dpos;
-      ++pos;
-      dpos += d[i];
-    }
+  while (take) {
+    const int64_t v = w * 32 + __ffs(take) - 1;
+    take &= take - 1;
+    const int64_t d = row_ptr[v + 1] - row_ptr[v];
+    queue[pos] = (int32_t)v;
+    qdeg[pos] = dpos;
+    ++pos;
+    dpos += d;
   }
 }
 
 // Top-down push for the roots in td_mask: edge-balanced over the queue rows
 // (each warp takes kBTile adjacency entries of the concatenated rows).  For
-// an edge (u, v) the bits f = planes[L-1][u] & td_mask not yet in seen[v]
-// are claimed with a fetch-OR on seen[v]; the bits this thread actually
-// claimed go into planes[L][v].  Every (root, vertex) pair is thus claimed
-// exactly once, by a parent at level L-1.
+// an edge (u, v) the bits m = planes[L-1][u] & td_mask not in seen[v] are
+// ORed (non-returning) into planes[L][v] and seen[v], and v is marked in the
+// touched-row bitmap.  seen[v] may be stale for bits set during this level;
+// those bits are new in level L all the same, so planes[L] still gets exactly
+// the (root, vertex) pairs first reached at level L.  Runs after the
+// bottom-up sweep of the level, which only writes bottom-up roots' bits.
 __global__ void __launch_bounds__(256) batch_td_kernel(
     BatchCtl* __restrict__ ctl, const int32_t* __restrict__ queue,
     const int64_t* __restrict__ qdeg, const int64_t* __restrict__ row_ptr,
@@ -248,6 +253,7 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   unsigned long long* cur = plane_ptr(ctl, L);
   unsigned long long* seen = ctl->seen;
+  uint32_t* rb = ctl->rowbits[L & 1];
   const int64_t total = qdeg[qsize];
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -284,15 +290,14 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
         f = prev[src] & T;
       }
       const int32_t u = __ldg(col + rbeg + (e - seg_lo));
-      // L2 read: seen changes during the kernel; a stale value only costs a
-      // fetch-OR that claims nothing
+      // L2 read: seen changes during the kernel; a stale value only costs
+      // redundant ORs
       const unsigned long long m = f & ~__ldcg(seen + u);
       if (m) {
-        const unsigned long long nw = m & ~atomicOr(seen + u, m);
-        if (nw) {
-          atomicOr(cur + u, nw);
-          found |= nw;
-        }
+        atomicOr(seen + u, m);
+        atomicOr(cur + u, m);
+        atomicOr(rb + (u >> 5), 1u << (u & 31));
+        found |= m;
       }
     }
   }
@@ -308,7 +313,9 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // neighbours per step, stopping as soon as U is covered.  Rows are sorted by
 // descending degree, so neighbour lists start with the hubs, which most
 // roots reach first.  The row's new bits are written to planes[L] and seen
-// by the lane that owns it: no atomics.  The frontier masks of level L-1 are
+// by the lane that owns it, and every row of planes[L] is written (zero when
+// nothing is found), before the top-down push of the level ORs into it: no
+// atomics.  The frontier masks of level L-1 are
 // only read here, and a bit of U can only come from a neighbour at level
 // L-1 of that root, so the OR over neighbours is exact.
 template <int kProbe>
@@ -319,10 +326,10 @@ __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ct
   const long long L = ctl->level;
   const int64_t R = ctl->R;
   const unsigned long long Bm = ctl->bu_mask_active;
-  const bool has_td = ctl->has_td != 0;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
   unsigned long long* __restrict__ seen = ctl->seen;
+  uint32_t* __restrict__ rb = ctl->rowbits[L & 1];
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -335,7 +342,7 @@ __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ct
     const unsigned long long U = ~s & Bm;
     const unsigned work = __ballot_sync(kFull, U != 0);
     if (!work) {
-      if (!has_td && valid) cur[v] = 0ull;
+      if (valid) cur[v] = 0ull;
       continue;
     }
     rows += (lane == 0) ? __popc(work) : 0;
@@ -384,10 +391,11 @@ __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ct
     }
     const unsigned long long n = acc & U;
     if (valid) {
-      if (!has_td) cur[v] = n;
-      else if (n) cur[v] |= n;
+      cur[v] = n;
       if (n) seen[v] = s | n;
     }
+    const unsigned hit = __ballot_sync(kFull, n != 0);
+    if (lane == 0 && hit) rb[ch] = hit;
     found |= n;
   }
   found = warp_or64(found);
@@ -485,6 +493,7 @@ __global__ void batch_control_kernel(BatchCtl* __restrict__ ctl, const int32_t* 
     if (r < 0) continue;
     cur[r] |= bit;
     c.seen[r] |= bit;
+    c.rowbits[L & 1][r >> 5] |= 1u << (r & 31);
     c.c.active |= bit;
     seeded |= bit;
   }
@@ -544,6 +553,7 @@ __global__ void batch_control_kernel(BatchCtl* __restrict__ ctl, const int32_t* 
 struct BatchSetupArg {
   unsigned long long* planes;
   unsigned long long* seen;
+  uint32_t* rowbits[2];
   long long R, capacity, nedges, nverts;
   double alpha, beta;
   int edgefactor, K;
@@ -551,9 +561,26 @@ struct BatchSetupArg {
   int lv[kBatchMax];       // its level
 };
 
+// seen = 0, planes[0] = 0 and the touched-row bitmap of level 0 = 0.
+__global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
+  const int64_t n = a->R;
+  unsigned long long* __restrict__ seen = a->seen;
+  unsigned long long* __restrict__ p0 = a->planes;
+  uint32_t* __restrict__ rb = a->rowbits[0];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    seen[i] = 0ull;
+    p0[i] = 0ull;
+  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31) >> 5);
+       i += stride)
+    rb[i] = 0u;
+}
+
 // Initialises the control block for a new batch (64 threads).
-__global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, BatchSetupArg a,
+__global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, const BatchSetupArg* __restrict__ ap,
                                    const int32_t* __restrict__ rank, int64_t nverts) {
+  const BatchSetupArg& a = *ap;
   const int t = threadIdx.x;
   if (t < kBatchMax) {
     const bool ok = t < a.K && a.v[t] >= 0 && a.v[t] < nverts;
@@ -564,6 +591,8 @@ __global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, BatchSetupArg a,
   if (t == 0) {
     ctl->planes = a.planes;
     ctl->seen = a.seen;
+    ctl->rowbits[0] = a.rowbits[0];
+    ctl->rowbits[1] = a.rowbits[1];
     ctl->R = a.R;
     ctl->capacity = a.capacity;
     ctl->nedges = a.nedges;
@@ -659,15 +688,26 @@ cudaEvent_t BatchState::event(size_t i) {
 void BatchState::release(DeviceArena& arena) {
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
   ev.clear();
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
+  graph_exec = nullptr;
+  graph = nullptr;
+  graph_key.clear();
   if (!allocated) return;
+  arena.free(d_arg);
+  cudaFreeHost(h_arg);
+  d_arg = h_arg = nullptr;
   arena.free(planes);
   arena.free(seen);
+  arena.free(rowbits[0]);
+  arena.free(rowbits[1]);
   arena.free(blk_cnt);
   arena.free(blk_deg);
   arena.free(ctl);
   cudaFreeHost(hctl);
   cudaFreeHost(hdone);
   planes = seen = nullptr;
+  rowbits[0] = rowbits[1] = nullptr;
   blk_cnt = blk_deg = nullptr;
   ctl = nullptr;
   hctl = nullptr;
@@ -683,13 +723,18 @@ namespace {
 void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
   bs.release(arena);
   bs.R = g.csr.nrows;
-  bs.nblk = (bs.R + kQBlockRows - 1) / kQBlockRows;
+  const int64_t W = (bs.R + 31) / 32;
+  bs.nblk = (W + kQThreads - 1) / kQThreads;
   bs.seen = arena_alloc<unsigned long long>(arena, bs.R, "batch seen masks");
+  bs.rowbits[0] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
+  bs.rowbits[1] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
   bs.blk_cnt = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block counts");
   bs.blk_deg = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block degrees");
   bs.ctl = arena_alloc<BatchCtl>(arena, 1, "batch control block");
   check_cuda(cudaMallocHost(&bs.hctl, sizeof(BatchCtl)), "pinned batch control");
   check_cuda(cudaMallocHost(&bs.hdone, sizeof(int)), "pinned flag");
+  bs.d_arg = arena_alloc<BatchSetupArg>(arena, 1, "batch arguments");
+  check_cuda(cudaMallocHost(&bs.h_arg, sizeof(BatchSetupArg)), "pinned batch arguments");
   bs.allocated = true;
   // Level planes: 16 to start with (Kronecker searches need about 10),
   // fewer when memory is short; the search grows the pool when it runs out.
@@ -719,12 +764,113 @@ void batch_grow(DeviceArena& arena, BatchState& bs, int64_t used, cudaStream_t s
 
 }  // namespace
 
+namespace {
+
+// The kernels of one level, in order.  With events, records the level's
+// start, end of queue building, end of the bottom-up sweep and end of the
+// top-down push at ev[0..3].
+void launch_level(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, int sms,
+                  cudaGraphConditionalHandle cond, int use_cond, const cudaEvent_t* ev) {
+  const Csr& c = g.csr;
+  const int B = 256;
+  const unsigned nblk = (unsigned)std::max<int64_t>(bs.nblk, 1);
+  if (ev) check_cuda(cudaEventRecord(ev[0], s), "event");
+  batch_clear_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.ctl);
+  batch_queue_count_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg);
+  batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, st.qdeg);
+  batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
+                                                      st.queue, st.qdeg);
+  if (ev) check_cuda(cudaEventRecord(ev[1], s), "event");
+  batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col);
+  if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
+  batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, st.queue, st.qdeg, c.row_ptr, c.col);
+  if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
+  batch_stats_kernel<<<sms * 2, B, 0, s>>>(bs.ctl, c.mdeg);
+  batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, cond, use_cond);
+}
+constexpr int kLevelLaunches = 8;
+
+void launch_prologue(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
+  batch_zero_kernel<<<grid_for(bs.R, 256, sms, 8), 256, 0, s>>>(
+      static_cast<const BatchSetupArg*>(bs.d_arg));
+  batch_setup_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, static_cast<const BatchSetupArg*>(bs.d_arg),
+                                             g.csr.rank, g.nverts);
+}
+
+std::vector<const void*> graph_key_of(const Graph& g, const BfsState& st, const BatchState& bs,
+                                      int sms) {
+  const Csr& c = g.csr;
+  return {bs.ctl, bs.d_arg, bs.blk_cnt, bs.blk_deg, (const void*)(intptr_t)bs.nblk,
+          (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, c.rank,
+          (const void*)(intptr_t)g.nverts, st.queue, st.qdeg, (const void*)(intptr_t)sms};
+}
+
+// Prologue (zero, setup, first control) followed by a WHILE node whose body
+// is one level; the control kernel sets the loop condition.
+void build_graph(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, int sms) {
+  if (bs.graph_exec) cudaGraphExecDestroy(bs.graph_exec);
+  if (bs.graph) cudaGraphDestroy(bs.graph);
+  bs.graph_exec = nullptr;
+  bs.graph = nullptr;
+  check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+  cudaGraph_t cg = nullptr;
+  cudaGraph_t body = nullptr;
+  cudaError_t err = cudaSuccess;
+  {
+    launch_prologue(g, bs, s, sms);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle cond = 0;
+    err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+    if (err == cudaSuccess)
+      err = cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault);
+    if (err == cudaSuccess) {
+      batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, g.csr.mdeg, cond, 1);
+      err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+    }
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = cond;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    if (err == cudaSuccess) err = cudaGraphAddNode(&node, cg, deps, nd, &p);
+    if (err == cudaSuccess)
+      err = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (err == cudaSuccess) body = p.conditional.phGraph_out[0];
+    cudaGraph_t outer = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s, &outer);
+    if (err == cudaSuccess) err = e2;
+    bs.graph = outer;
+    if (err == cudaSuccess) {
+      err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+      if (err == cudaSuccess) {
+        launch_level(g, st, bs, s, sms, cond, 1, nullptr);
+        cudaGraph_t b2 = nullptr;
+        err = cudaStreamEndCapture(s, &b2);
+      }
+    }
+  }
+  if (err == cudaSuccess) err = cudaGraphInstantiate(&bs.graph_exec, bs.graph, 0);
+  if (err != cudaSuccess) {
+    if (bs.graph) cudaGraphDestroy(bs.graph);
+    bs.graph = nullptr;
+    bs.graph_exec = nullptr;
+    cudaGetLastError();
+    check_cuda(err, "batch level-loop graph");
+  }
+  bs.graph_key = graph_key_of(g, st, bs, sms);
+}
+
+}  // namespace
+
 void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
-               b200bfs_batch_stats* stats) {
+               bool use_graph, b200bfs_batch_stats* stats) {
   const Csr& c = g.csr;
   if (!bs.allocated || bs.R != c.nrows) batch_allocate(arena, g, bs);
-  BatchSetupArg a;
+  BatchSetupArg& a = *static_cast<BatchSetupArg*>(bs.h_arg);
   memset(&a, 0, sizeof(a));
   bs.roots.assign(roots, roots + k);
   bs.entry_vertex.assign((size_t)k, -1);
@@ -741,6 +887,8 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
   }
   a.planes = bs.planes;
   a.seen = bs.seen;
+  a.rowbits[0] = bs.rowbits[0];
+  a.rowbits[1] = bs.rowbits[1];
   a.R = bs.R;
   a.capacity = bs.capacity;
   a.nedges = c.nedges;
@@ -751,41 +899,48 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
   a.K = k;
   bs.K = k;
 
-  const int B = 256;
+  if (use_graph && (!bs.graph_exec || bs.graph_key != graph_key_of(g, st, bs, sms)))
+    build_graph(g, st, bs, s, sms);
+
   size_t nev = 0;
   check_cuda(cudaEventRecord(bs.event(nev++), s), "event");
-  batch_zero_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.seen, bs.planes, bs.R);
-  batch_setup_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, a, c.rank, g.nverts);
-  batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
-  int launches = 3;
-  const unsigned nblk = (unsigned)std::max<int64_t>(bs.nblk, 1);
-  std::vector<std::pair<size_t, size_t>> bu_ev;
-  for (;;) {
-    batch_queue_count_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg);
-    batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, st.qdeg);
-    batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt,
-                                                        bs.blk_deg, st.queue, st.qdeg);
-    batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, st.queue, st.qdeg, c.row_ptr, c.col);
-    check_cuda(cudaEventRecord(bs.event(nev), s), "event");
-    batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col);
-    check_cuda(cudaEventRecord(bs.event(nev + 1), s), "event");
-    bu_ev.push_back({nev, nev + 1});
-    nev += 2;
-    batch_stats_kernel<<<sms * 2, B, 0, s>>>(bs.ctl, c.mdeg);
+  check_cuda(cudaMemcpyAsync(bs.d_arg, bs.h_arg, sizeof(BatchSetupArg), cudaMemcpyHostToDevice, s),
+             "batch arguments");
+  int launches;
+  bool loop_on_host = !use_graph;
+  if (use_graph) {
+    check_cuda(cudaGraphLaunch(bs.graph_exec, s), "batch graph");
+    launches = 3;  // per level below
+  } else {
+    launch_prologue(g, bs, s, sms);
     batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
-    launches += 7;
+    launches = 3;
+  }
+  // per level on the host: start, queue built, bottom-up done, top-down done
+  std::vector<size_t> lev_ev;
+  for (;;) {
+    if (loop_on_host) {
+      lev_ev.push_back(nev);
+      cudaEvent_t e4[4] = {bs.event(nev), bs.event(nev + 1), bs.event(nev + 2), bs.event(nev + 3)};
+      nev += 4;
+      launch_level(g, st, bs, s, sms, 0, 0, e4);
+    }
     check_cuda(cudaMemcpyAsync(bs.hdone, &bs.ctl->done, sizeof(int), cudaMemcpyDeviceToHost, s),
                "batch flag");
     check_cuda(cudaStreamSynchronize(s), "batch level");
     const int done = *bs.hdone;
-    if (done == 0) continue;
+    if (done == 0) {
+      loop_on_host = true;
+      continue;
+    }
     if (done == 1) break;
     if (done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
-    // done == 2: the next level needs another plane
+    // done == 2: the next level needs another plane; the host loop resumes
     check_cuda(cudaMemcpyAsync(bs.hctl, bs.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s),
                "batch control");
     check_cuda(cudaStreamSynchronize(s), "batch control");
     batch_grow(arena, bs, bs.hctl->level, s);
+    loop_on_host = true;
     ++launches;
   }
   check_cuda(cudaEventRecord(bs.event(nev++), s), "event");
@@ -796,41 +951,54 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
   const BatchCtl& h = *bs.hctl;
   // the last level found nothing: planes [0, level) hold the levels
   bs.levels = h.level;
-  if (stats) {
-    b200bfs_batch_stats r;
-    memset(&r, 0, sizeof(r));
-    r.num_roots = k;
-    r.levels = (int32_t)std::max<long long>(h.level - 1, 0);
-    r.kernel_launches = launches;
-    const int64_t R = bs.R;
-    int64_t bytes = 16 * R;  // seen and plane 0
-    for (long long L = 1; L <= h.level && L < kBatchHist; ++L) {
-      const BatchLevelRec& x = h.hist[L];
-      if (x.td_roots) {
-        ++r.num_td_levels;
-        r.edges_scanned_td += (int64_t)x.qedges;
-        bytes += 16 * (int64_t)x.qsize + 12 * (int64_t)x.qedges;
-      }
-      if (x.bu_roots) {
-        ++r.num_bu_levels;
-        r.edges_scanned_bu += (int64_t)x.scanned_bu;
-        const int64_t b = 16 * R + 16 * (int64_t)x.rows_bu + 12 * (int64_t)x.scanned_bu;
-        r.bu_bytes += b;
-        bytes += b;
-      } else {
-        bytes += 8 * R;  // the level's plane
-      }
+  b200bfs_batch_stats r;
+  memset(&r, 0, sizeof(r));
+  r.num_roots = k;
+  r.levels = (int32_t)std::max<long long>(h.level - 1, 0);
+  r.kernel_launches = launches + kLevelLaunches * (int)h.level;
+  const int64_t R = bs.R;
+  int64_t bytes = 16 * R;  // seen and plane 0
+  st.levels.clear();
+  // host-loop levels carry events; levels run inside the graph do not
+  const long long first_host_level = (long long)h.level + 1 - (long long)lev_ev.size();
+  for (long long L = 1; L <= h.level && L < kBatchHist; ++L) {
+    const BatchLevelRec& x = h.hist[L];
+    float td_ms = 0, bu_ms = 0, push_ms = 0;
+    if (L >= first_host_level) {
+      const size_t ea = lev_ev[(size_t)(L - first_host_level)];
+      check_cuda(cudaEventElapsedTime(&td_ms, bs.ev[ea], bs.ev[ea + 1]), "elapsed");
+      check_cuda(cudaEventElapsedTime(&bu_ms, bs.ev[ea + 1], bs.ev[ea + 2]), "elapsed");
+      check_cuda(cudaEventElapsedTime(&push_ms, bs.ev[ea + 2], bs.ev[ea + 3]), "elapsed");
+      td_ms += push_ms;
     }
-    r.algorithmic_bytes = bytes;
-    float ms = 0;
-    check_cuda(cudaEventElapsedTime(&ms, bs.ev[0], bs.ev[nev - 1]), "elapsed");
-    r.ms = ms;
-    for (const auto& p : bu_ev) {
-      check_cuda(cudaEventElapsedTime(&ms, bs.ev[p.first], bs.ev[p.second]), "elapsed");
-      r.bu_ms += ms;
+    if (x.td_roots) {
+      ++r.num_td_levels;
+      r.edges_scanned_td += (int64_t)x.qedges;
+      // rows + entries + seen probes
+      const int64_t b = 16 * (int64_t)x.qsize + 12 * (int64_t)x.qedges;
+      bytes += b;
+      r.td_ms += td_ms;
+      st.levels.push_back({(int32_t)L, 0, (int64_t)x.qsize, __builtin_popcountll(x.td_roots),
+                           (int64_t)x.qedges, b, td_ms});
     }
-    *stats = r;
+    if (x.bu_roots) {
+      ++r.num_bu_levels;
+      r.edges_scanned_bu += (int64_t)x.scanned_bu;
+      const int64_t b = 16 * R + 16 * (int64_t)x.rows_bu + 12 * (int64_t)x.scanned_bu;
+      r.bu_bytes += b;
+      bytes += b;
+      r.bu_ms += bu_ms;
+      st.levels.push_back({(int32_t)L, 1, (int64_t)x.rows_bu, __builtin_popcountll(x.bu_roots),
+                           (int64_t)x.scanned_bu, b, bu_ms});
+    } else {
+      bytes += 8 * R;  // the level's plane
+    }
   }
+  r.algorithmic_bytes = bytes;
+  float ms = 0;
+  check_cuda(cudaEventElapsedTime(&ms, bs.ev[0], bs.ev[nev - 1]), "elapsed");
+  r.ms = ms;
+  if (stats) *stats = r;
 }
 
 void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream_t s, int sms,

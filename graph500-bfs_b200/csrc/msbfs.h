@@ -38,6 +38,7 @@ struct BatchCtl {
   // fixed during a search
   unsigned long long* planes;  // [capacity][R]: bit k of planes[L][v] <=> level_k(v) == L
   unsigned long long* seen;    // [R]: bits of the roots that reached v
+  uint32_t* rowbits[2];        // [R/32]: rows with a bit in planes[L], for L even / odd
   long long R;
   long long capacity;          // planes allocated
   long long nedges;            // num_global_edges (alpha test)
@@ -68,12 +69,21 @@ struct BatchState {
   int64_t nblk = 0;
   unsigned long long* planes = nullptr;
   unsigned long long* seen = nullptr;
+  uint32_t* rowbits[2] = {nullptr, nullptr};
   int64_t* blk_cnt = nullptr;
   int64_t* blk_deg = nullptr;
   BatchCtl* ctl = nullptr;   // device
   BatchCtl* hctl = nullptr;  // pinned mirror
   int* hdone = nullptr;      // pinned copy of ctl->done
+  void* d_arg = nullptr;     // device copy of the batch arguments
+  void* h_arg = nullptr;     // pinned staging of the batch arguments
   std::vector<cudaEvent_t> ev;
+  // The level loop as one CUDA graph (a WHILE conditional node around the
+  // level kernels), built on first use and rebuilt when a buffer it names
+  // changes.
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<const void*> graph_key;
   // last batch
   int K = 0;
   int64_t levels = 0;                 // planes in use = last level + 1
@@ -86,11 +96,13 @@ struct BatchState {
 };
 
 // Runs one batched search from roots[0..k) over g.csr.  alpha <= 0 selects
-// kBatchAlpha.  The CoreBFS climb of each root is applied as in
+// kBatchAlpha.  use_graph: run the level loop as a CUDA graph on the device
+// (one host synchronisation per batch); otherwise the host launches each
+// level and records per-level timings.  The CoreBFS climb of each root is applied as in
 // BfsBase::run_bfs (bfs.hpp:3214-3232).
 void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
-               b200bfs_batch_stats* stats);
+               bool use_graph, b200bfs_batch_stats* stats);
 
 // Writes root `index` of the last batch into st.pred in the reference
 // encoding: level from the planes, parent = a neighbour one level closer to

@@ -130,6 +130,7 @@ typedef struct b200bfs_batch_stats {
   int64_t bu_bytes;              /* of which in the bottom-up kernel          */
   double ms;                     /* CUDA-event time of the whole batch        */
   double bu_ms;                  /* CUDA-event time of the bottom-up kernels  */
+  double td_ms;                  /* CUDA-event time of the top-down parts     */
 } b200bfs_batch_stats;
 
 /* --------------------------- lifetime / errors --------------------------- */
@@ -231,8 +232,10 @@ int b200bfs_get_pred(b200bfs_handle* h, int64_t* pred);
  * levels of CoreBFS tree vertices filled in: levels[pred_size]. */
 int b200bfs_get_levels(b200bfs_handle* h, int32_t* levels);
 
-/* Per-level records of the last run: up to max entries into out, the
- * number of levels in *count. */
+/* Per-level records of the last run or batch (a batch level with both a
+ * top-down and a bottom-up part gives two records; there `discovered` is the
+ * number of roots in that part): up to max entries into out, the number of
+ * records in *count. */
 int b200bfs_get_level_stats(b200bfs_handle* h, b200bfs_level_stats* out, int max, int* count);
 
 /* Statistics of the last run. */
@@ -242,8 +245,12 @@ int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
  * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
  * kernel form), "td_kernel" (1..2, top-down kernel form), "bu_probe" (1..64,
  * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
- * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2).  None of
- * them changes levels or the validity of parents. */
+ * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2),
+ * "batch_graph" (1: b200bfs_run_batch runs its level loop as a CUDA graph on
+ * the device, 0: the host launches each level and per-level times are
+ * recorded), "batch_alpha" (the alpha b200bfs_run_batch uses when given
+ * alpha <= 0; default 30).  None of them changes levels or the validity of
+ * parents. */
 int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value);
 
 /* The CUDA stream (a cudaStream_t) the engine launches its kernels on, for
@@ -272,7 +279,7 @@ int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors,
  * that reached it, so one read of an adjacency row serves all roots.  Each
  * root switches between top-down and bottom-up on its own, with the rule of
  * bfs.hpp:3413-3457 applied to that root's frontier (alpha <= 0 selects the
- * batch default 30; beta as for b200bfs_run).  Per-root levels equal those
+ * engine's "batch_alpha" option, default 30; beta as for b200bfs_run).  Per-root levels equal those
  * of b200bfs_run from the same root.  Requires b200bfs_prepare; with CoreBFS
  * each root climbs to the 2-core first, as b200bfs_run does.  stats may be
  * NULL. */

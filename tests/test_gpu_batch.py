@@ -79,6 +79,27 @@ def test_batch_any_direction_gives_same_levels(engine, graphs, alpha):
         assert st.num_bu_levels > 0
 
 
+def test_batch_host_loop_and_graph_agree(engine, graphs):
+    """The level loop run by the host (with per-level timings) and as a CUDA
+    graph on the device give the same levels and statistics."""
+    edges, g = graphs(16)
+    engine.generate_graph(16, 16)
+    engine.prepare(16)
+    roots = O.find_roots(g.has_edge(), 1 << 16, 64)
+    try:
+        engine.set_option("batch_graph", 0)
+        a = _check_batch(engine, edges, g, roots)
+        lv = engine.level_stats()
+        assert lv and all(x["ms"] > 0 for x in lv)
+        engine.set_option("batch_graph", 1)
+        b = _check_batch(engine, edges, g, roots)
+    finally:
+        engine.set_option("batch_graph", 1)
+    for f in ("levels", "num_td_levels", "num_bu_levels", "edges_scanned_td", "edges_scanned_bu",
+              "algorithmic_bytes"):
+        assert getattr(a, f) == getattr(b, f), f
+
+
 def test_batch_duplicate_and_isolated_roots(engine, graphs):
     edges, g = graphs(14)
     engine.generate_graph(14, 16)
