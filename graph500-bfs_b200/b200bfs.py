@@ -40,7 +40,12 @@ SYMBOLS = [
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
     "b200bfs_validate", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
+    "b200bfs_server_start", "b200bfs_server_add_graph", "b200bfs_server_graph_info",
+    "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
+    "b200bfs_server_get_levels", "b200bfs_server_release", "b200bfs_server_get_stats",
+    "b200bfs_server_reset_stats", "b200bfs_server_last_error", "b200bfs_server_stop",
 ]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(5)
 BATCH_MAX = 64  # B200BFS_BATCH_MAX
 BATCH_ALPHA = 30.0  # batch default of the top-down -> bottom-up threshold
 
@@ -98,6 +103,32 @@ class BatchStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("slots_per_graph", ctypes.c_int), ("keep_results", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_uint64), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("graph_id", ctypes.c_int32),
+                ("root", ctypes.c_int64), ("depth", ctypes.c_int32),
+                ("batch_size", ctypes.c_int32), ("latency_ms", ctypes.c_double),
+                ("queue_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64),
+                ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("mean_batch_size", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("bfs_per_s", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
+                ("graphs", ctypes.c_int32), ("slots", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -140,6 +171,20 @@ def load_library(path=LIB_PATH):
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
     L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
     L.b200bfs_batch_select.argtypes = [H, i32]
+    S = ctypes.c_void_p
+    L.b200bfs_server_start.argtypes = [P(ServerConfig), P(S)]
+    L.b200bfs_server_add_graph.argtypes = [S, i32, i32, u64, u64, i32, P(ctypes.c_int)]
+    L.b200bfs_server_graph_info.argtypes = [S, i32, P(GraphInfo)]
+    L.b200bfs_server_submit.argtypes = [S, i32, i64, P(ctypes.c_int64)]
+    L.b200bfs_server_poll.argtypes = [S, i64, P(RequestInfo)]
+    L.b200bfs_server_wait.argtypes = [S, i64, dbl, P(RequestInfo)]
+    L.b200bfs_server_get_levels.argtypes = [S, i64, vp]
+    L.b200bfs_server_release.argtypes = [S, i64]
+    L.b200bfs_server_get_stats.argtypes = [S, P(ServerStats)]
+    L.b200bfs_server_reset_stats.argtypes = [S]
+    L.b200bfs_server_last_error.argtypes = [S]
+    L.b200bfs_server_last_error.restype = ctypes.c_char_p
+    L.b200bfs_server_stop.argtypes = [S]
     _lib = L
     return L
 
@@ -323,6 +368,79 @@ def bfs_noalloc(row_ptr_dev, col_dev, nrows, root, pred_dev, stream=0):
     if rc != OK:
         raise B200BfsError(rc, "b200bfs_bfs_noalloc failed")
     return nl.value
+
+
+class Server:
+    """BFS server with continuous batching (b200bfs_server_*): graphs stay
+    resident on the device and (graph, root) queries are answered as they
+    arrive, packed into batched searches by per-slot worker threads."""
+
+    def __init__(self, device=0, max_batch=64, slots_per_graph=2, keep_results=False,
+                 hbm_budget_bytes=0, alpha=0.0, beta=0.0):
+        self.L = load_library()
+        cfg = ServerConfig(device, max_batch, slots_per_graph, int(bool(keep_results)),
+                           hbm_budget_bytes, alpha, beta)
+        self.s = ctypes.c_void_p()
+        rc = self.L.b200bfs_server_start(ctypes.byref(cfg), ctypes.byref(self.s))
+        if rc != OK:
+            raise B200BfsError(rc, "b200bfs_server_start failed")
+
+    def check(self, rc):
+        if rc != OK:
+            raise B200BfsError(rc, self.L.b200bfs_server_last_error(self.s).decode())
+
+    def add_graph(self, scale, edgefactor=16, seed1=USERSEED1, seed2=USERSEED2, flags=0):
+        gid = ctypes.c_int()
+        self.check(self.L.b200bfs_server_add_graph(self.s, scale, edgefactor, seed1, seed2, flags,
+                                                   ctypes.byref(gid)))
+        return gid.value
+
+    def graph_info(self, gid):
+        gi = GraphInfo()
+        self.check(self.L.b200bfs_server_graph_info(self.s, gid, ctypes.byref(gi)))
+        return gi
+
+    def submit(self, gid, root):
+        rid = ctypes.c_int64()
+        self.check(self.L.b200bfs_server_submit(self.s, gid, int(root), ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, rid):
+        info = RequestInfo()
+        self.check(self.L.b200bfs_server_poll(self.s, rid, ctypes.byref(info)))
+        return info
+
+    def wait(self, rid, timeout=60.0):
+        info = RequestInfo()
+        self.check(self.L.b200bfs_server_wait(self.s, rid, timeout, ctypes.byref(info)))
+        return info
+
+    def levels(self, rid, pred_size):
+        out = np.empty(pred_size, dtype=np.int32)
+        self.check(self.L.b200bfs_server_get_levels(self.s, rid, _ptr(out)))
+        return out
+
+    def release(self, rid):
+        self.check(self.L.b200bfs_server_release(self.s, rid))
+
+    def stats(self):
+        st = ServerStats()
+        self.check(self.L.b200bfs_server_get_stats(self.s, ctypes.byref(st)))
+        return st
+
+    def reset_stats(self):
+        self.check(self.L.b200bfs_server_reset_stats(self.s))
+
+    def stop(self):
+        if self.s:
+            self.L.b200bfs_server_stop(self.s)
+            self.s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 class _GraphFacade:

@@ -11,6 +11,7 @@
 #include "validate.h"
 #include "autotune.h"
 #include "msbfs.h"
+#include "engine_state.h"
 
 namespace b200bfs {
 
@@ -24,12 +25,21 @@ void check_cuda(cudaError_t e, const char* what) {
 
 void* DeviceArena::alloc(size_t bytes, const char* what) {
   if (bytes == 0) bytes = 16;
+  std::lock_guard<std::mutex> lock(mu_);
   if (budget_ && in_use_ + bytes > budget_)
     throw Error{B200BFS_ERR_OOM, std::string("HBM budget exceeded allocating ") + what};
+  if (shared_) {
+    const uint64_t before = shared_->used.fetch_add(bytes);
+    if (shared_->limit && before + bytes > shared_->limit) {
+      shared_->used.fetch_sub(bytes);
+      throw Error{B200BFS_ERR_OOM, std::string("shared HBM budget exceeded allocating ") + what};
+    }
+  }
   void* p = nullptr;
   cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    if (shared_) shared_->used.fetch_sub(bytes);
     throw Error{B200BFS_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" +
                                      std::to_string(bytes) + " bytes)"};
   }
@@ -40,9 +50,11 @@ void* DeviceArena::alloc(size_t bytes, const char* what) {
 
 void DeviceArena::free(void* p) {
   if (!p) return;
+  std::lock_guard<std::mutex> lock(mu_);
   for (size_t i = 0; i < live_.size(); ++i)
     if (live_[i].p == p) {
       in_use_ -= live_[i].bytes;
+      if (shared_) shared_->used.fetch_sub(live_[i].bytes);
       live_[i] = live_.back();
       live_.pop_back();
       cudaFree(p);
@@ -51,9 +63,11 @@ void DeviceArena::free(void* p) {
 }
 
 void DeviceArena::rollback(uint64_t m) {
+  std::lock_guard<std::mutex> lock(mu_);
   for (size_t i = 0; i < live_.size();) {
     if (live_[i].seq >= m) {
       in_use_ -= live_[i].bytes;
+      if (shared_) shared_->used.fetch_sub(live_[i].bytes);
       cudaFree(live_[i].p);
       live_[i] = live_.back();
       live_.pop_back();
@@ -91,74 +105,11 @@ __global__ void packed_to_uint2_kernel(const uint32_t* __restrict__ in, int64_t 
 using detail_io::pairs_to_uint2_kernel;
 using detail_io::packed_to_uint2_kernel;
 
-struct Engine {
-  int device = 0;
-  int sms = 148;
-  cudaStream_t stream = nullptr;
-  DeviceArena arena;
-  Graph g;
-  BfsState st;
-  BatchState bs;
-  bool prepared = false;
-  bool have_run = false;
-  int64_t last_root = -1;
-  b200bfs_run_stats last_stats{};
-  RunOptions opt;
-  std::string last_error = "no error";
-
-  void free_graph() {
-    if (st.allocated) st.release(arena);
-    bs.release(arena);
-    prepared = false;
-    have_run = false;
-    free_core(arena, g);
-    arena.free(g.csr.row_ptr);
-    arena.free(g.csr.col);
-    arena.free(g.csr.inv);
-    arena.free(g.csr.rank);
-    arena.free(g.csr.mdeg);
-    arena.free(g.input_edges);
-    g = Graph();
-  }
-
-  void finish_build(uint2* d_edges, int64_t m, int scale_hint, int flags) {
-    const bool mirror = !(flags & B200BFS_BUILD_INPUT_SYMMETRIC);
-    g.input_edges = d_edges;
-    g.num_input_edges = m;
-    g.input_symmetric = !mirror;
-    build_csr(arena, stream, d_edges, m, mirror, (flags & B200BFS_BUILD_GROUP_REORDER) != 0,
-              scale_hint, g, sms);
-    if (flags & B200BFS_BUILD_COREBFS) build_core(arena, stream, g, sms);
-    g.built = true;
-    g.device_bytes = (int64_t)arena.in_use();
-  }
-
-  // Runs a graph build; on failure every allocation of the build is released
-  // and the handle is left without a graph.
-  template <typename F>
-  void build_guarded(F&& f) {
-    free_graph();
-    const uint64_t m = arena.mark();
-    try {
-      f();
-    } catch (...) {
-      cudaStreamSynchronize(stream);
-      cudaGetLastError();
-      arena.rollback(m);
-      g = Graph();
-      throw;
-    }
-  }
-};
-
 }  // namespace b200bfs
 
 using b200bfs::Engine;
 using b200bfs::Error;
 
-struct b200bfs_handle {
-  Engine e;
-};
 
 namespace {
 
@@ -636,8 +587,9 @@ int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, in
     for (int i = 0; i < num_roots; ++i)
       require(roots[i] >= 0 && roots[i] < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
     b200bfs_batch_stats rs;
-    b200bfs::run_batch(e.arena, e.g, e.st, e.bs, e.stream, e.sms, roots, num_roots, edgefactor,
+    b200bfs::run_batch(e.arena, e.g, e.bs, e.stream, e.sms, roots, num_roots, edgefactor,
                        alpha > 0 ? alpha : e.opt.batch_alpha, beta, e.opt.batch_graph != 0, &rs);
+    e.st.levels = e.bs.level_records;
     if (stats) *stats = rs;
     e.have_run = false;
   });

@@ -1,7 +1,9 @@
 // Internal interfaces of the B200 BFS engine (not part of the C ABI).
 #pragma once
 
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -27,12 +29,20 @@ struct Error {
   std::string msg;
 };
 
-// Device memory with an optional budget (b200bfs_config.hbm_budget_bytes).
-// Allocations carry a sequence number so that a failed build can release
-// everything it allocated (mark / rollback).
+// A device-memory budget shared by several arenas (the graphs of a server).
+struct SharedBudget {
+  uint64_t limit = 0;
+  std::atomic<uint64_t> used{0};
+};
+
+// Device memory with an optional budget (b200bfs_config.hbm_budget_bytes)
+// and an optional budget shared with other arenas.  Allocations carry a
+// sequence number so that a failed build can release everything it
+// allocated (mark / rollback).  Thread-safe.
 class DeviceArena {
  public:
   explicit DeviceArena(uint64_t budget = 0) : budget_(budget) {}
+  void set_shared(SharedBudget* sb) { shared_ = sb; }
   void* alloc(size_t bytes, const char* what);  // throws Error
   void free(void* p);
   uint64_t mark() const { return seq_; }
@@ -51,6 +61,8 @@ class DeviceArena {
   uint64_t in_use_ = 0;
   uint64_t seq_ = 0;
   std::vector<Block> live_;
+  SharedBudget* shared_ = nullptr;
+  std::mutex mu_;
 };
 
 template <typename T>

@@ -701,6 +701,10 @@ void BatchState::release(DeviceArena& arena) {
   arena.free(seen);
   arena.free(rowbits[0]);
   arena.free(rowbits[1]);
+  arena.free(queue);
+  arena.free(qdeg);
+  queue = nullptr;
+  qdeg = nullptr;
   arena.free(blk_cnt);
   arena.free(blk_deg);
   arena.free(ctl);
@@ -728,6 +732,8 @@ void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
   bs.seen = arena_alloc<unsigned long long>(arena, bs.R, "batch seen masks");
   bs.rowbits[0] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
   bs.rowbits[1] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
+  bs.queue = arena_alloc<int32_t>(arena, bs.R + 1, "batch frontier queue");
+  bs.qdeg = arena_alloc<int64_t>(arena, bs.R + 2, "batch frontier degree prefix");
   bs.blk_cnt = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block counts");
   bs.blk_deg = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block degrees");
   bs.ctl = arena_alloc<BatchCtl>(arena, 1, "batch control block");
@@ -769,7 +775,7 @@ namespace {
 // The kernels of one level, in order.  With events, records the level's
 // start, end of queue building, end of the bottom-up sweep and end of the
 // top-down push at ev[0..3].
-void launch_level(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, int sms,
+void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
                   cudaGraphConditionalHandle cond, int use_cond, const cudaEvent_t* ev) {
   const Csr& c = g.csr;
   const int B = 256;
@@ -777,13 +783,13 @@ void launch_level(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, 
   if (ev) check_cuda(cudaEventRecord(ev[0], s), "event");
   batch_clear_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.ctl);
   batch_queue_count_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg);
-  batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, st.qdeg);
+  batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, bs.qdeg);
   batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
-                                                      st.queue, st.qdeg);
+                                                      bs.queue, bs.qdeg);
   if (ev) check_cuda(cudaEventRecord(ev[1], s), "event");
   batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col);
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
-  batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, st.queue, st.qdeg, c.row_ptr, c.col);
+  batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg, c.row_ptr, c.col);
   if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
   batch_stats_kernel<<<sms * 2, B, 0, s>>>(bs.ctl, c.mdeg);
   batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, cond, use_cond);
@@ -797,17 +803,16 @@ void launch_prologue(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
                                              g.csr.rank, g.nverts);
 }
 
-std::vector<const void*> graph_key_of(const Graph& g, const BfsState& st, const BatchState& bs,
-                                      int sms) {
+std::vector<const void*> graph_key_of(const Graph& g, const BatchState& bs, int sms) {
   const Csr& c = g.csr;
   return {bs.ctl, bs.d_arg, bs.blk_cnt, bs.blk_deg, (const void*)(intptr_t)bs.nblk,
           (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, c.rank,
-          (const void*)(intptr_t)g.nverts, st.queue, st.qdeg, (const void*)(intptr_t)sms};
+          (const void*)(intptr_t)g.nverts, bs.queue, bs.qdeg, (const void*)(intptr_t)sms};
 }
 
 // Prologue (zero, setup, first control) followed by a WHILE node whose body
 // is one level; the control kernel sets the loop condition.
-void build_graph(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, int sms) {
+void build_graph(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
   if (bs.graph_exec) cudaGraphExecDestroy(bs.graph_exec);
   if (bs.graph) cudaGraphDestroy(bs.graph);
   bs.graph_exec = nullptr;
@@ -846,7 +851,7 @@ void build_graph(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, i
       err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeThreadLocal);
       if (err == cudaSuccess) {
-        launch_level(g, st, bs, s, sms, cond, 1, nullptr);
+        launch_level(g, bs, s, sms, cond, 1, nullptr);
         cudaGraph_t b2 = nullptr;
         err = cudaStreamEndCapture(s, &b2);
       }
@@ -860,12 +865,16 @@ void build_graph(const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s, i
     cudaGetLastError();
     check_cuda(err, "batch level-loop graph");
   }
-  bs.graph_key = graph_key_of(g, st, bs, sms);
+  bs.graph_key = graph_key_of(g, bs, sms);
 }
 
 }  // namespace
 
-void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
+void batch_reserve(DeviceArena& arena, const Graph& g, BatchState& bs) {
+  batch_allocate(arena, g, bs);
+}
+
+void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t s,
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
                bool use_graph, b200bfs_batch_stats* stats) {
   const Csr& c = g.csr;
@@ -899,8 +908,8 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
   a.K = k;
   bs.K = k;
 
-  if (use_graph && (!bs.graph_exec || bs.graph_key != graph_key_of(g, st, bs, sms)))
-    build_graph(g, st, bs, s, sms);
+  if (use_graph && (!bs.graph_exec || bs.graph_key != graph_key_of(g, bs, sms)))
+    build_graph(g, bs, s, sms);
 
   size_t nev = 0;
   check_cuda(cudaEventRecord(bs.event(nev++), s), "event");
@@ -923,7 +932,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
       lev_ev.push_back(nev);
       cudaEvent_t e4[4] = {bs.event(nev), bs.event(nev + 1), bs.event(nev + 2), bs.event(nev + 3)};
       nev += 4;
-      launch_level(g, st, bs, s, sms, 0, 0, e4);
+      launch_level(g, bs, s, sms, 0, 0, e4);
     }
     check_cuda(cudaMemcpyAsync(bs.hdone, &bs.ctl->done, sizeof(int), cudaMemcpyDeviceToHost, s),
                "batch flag");
@@ -958,7 +967,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
   r.kernel_launches = launches + kLevelLaunches * (int)h.level;
   const int64_t R = bs.R;
   int64_t bytes = 16 * R;  // seen and plane 0
-  st.levels.clear();
+  bs.level_records.clear();
   // host-loop levels carry events; levels run inside the graph do not
   const long long first_host_level = (long long)h.level + 1 - (long long)lev_ev.size();
   for (long long L = 1; L <= h.level && L < kBatchHist; ++L) {
@@ -978,7 +987,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
       const int64_t b = 16 * (int64_t)x.qsize + 12 * (int64_t)x.qedges;
       bytes += b;
       r.td_ms += td_ms;
-      st.levels.push_back({(int32_t)L, 0, (int64_t)x.qsize, __builtin_popcountll(x.td_roots),
+      bs.level_records.push_back({(int32_t)L, 0, (int64_t)x.qsize, __builtin_popcountll(x.td_roots),
                            (int64_t)x.qedges, b, td_ms});
     }
     if (x.bu_roots) {
@@ -988,7 +997,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs,
       r.bu_bytes += b;
       bytes += b;
       r.bu_ms += bu_ms;
-      st.levels.push_back({(int32_t)L, 1, (int64_t)x.rows_bu, __builtin_popcountll(x.bu_roots),
+      bs.level_records.push_back({(int32_t)L, 1, (int64_t)x.rows_bu, __builtin_popcountll(x.bu_roots),
                            (int64_t)x.scanned_bu, b, bu_ms});
     } else {
       bytes += 8 * R;  // the level's plane
@@ -1005,7 +1014,7 @@ void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream
                   int index) {
   const Csr& c = g.csr;
   const int B = 256;
-  int32_t* lv = st.queue;  // scratch of R + 1 entries
+  int32_t* lv = st.queue;  // scratch of R + 1 entries (the single-source queue)
   batch_row_levels_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.planes, bs.R, bs.levels,
                                                                  index, lv);
   fill_minus_one_kernel<<<grid_for(st.pred_size, B, sms, 8), B, 0, s>>>(st.pred, st.pred_size);

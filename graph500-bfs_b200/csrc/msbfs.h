@@ -70,6 +70,8 @@ struct BatchState {
   unsigned long long* planes = nullptr;
   unsigned long long* seen = nullptr;
   uint32_t* rowbits[2] = {nullptr, nullptr};
+  int32_t* queue = nullptr;  // top-down queue rows
+  int64_t* qdeg = nullptr;   // its degree prefix
   int64_t* blk_cnt = nullptr;
   int64_t* blk_deg = nullptr;
   BatchCtl* ctl = nullptr;   // device
@@ -91,6 +93,7 @@ struct BatchState {
   std::vector<int64_t> entry_vertex;  // vertex where each root enters the searched graph
   std::vector<int32_t> entry_level;   // level of that vertex (CoreBFS climb length)
   std::vector<std::vector<int64_t>> path_v, path_e;  // CoreBFS climb of each root
+  std::vector<b200bfs_level_stats> level_records;   // per level of the last batch
   cudaEvent_t event(size_t i);
   void release(DeviceArena& arena);
 };
@@ -100,9 +103,15 @@ struct BatchState {
 // (one host synchronisation per batch); otherwise the host launches each
 // level and records per-level timings.  The CoreBFS climb of each root is applied as in
 // BfsBase::run_bfs (bfs.hpp:3214-3232).
-void run_batch(DeviceArena& arena, const Graph& g, BfsState& st, BatchState& bs, cudaStream_t s,
+// A BatchState shares nothing mutable with other BatchStates of the same
+// graph, so batches on different states and streams may run concurrently.
+void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t s,
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
                bool use_graph, b200bfs_batch_stats* stats);
+
+// Allocates bs for g (level planes, masks, queue, control block) ahead of
+// its first batch.
+void batch_reserve(DeviceArena& arena, const Graph& g, BatchState& bs);
 
 // Writes root `index` of the last batch into st.pred in the reference
 // encoding: level from the planes, parent = a neighbour one level closer to

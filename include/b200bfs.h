@@ -292,6 +292,95 @@ int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, in
  * b200bfs_get_levels and b200bfs_validate then report that root. */
 int b200bfs_batch_select(b200bfs_handle* h, int index);
 
+/* -------------------------------- serving --------------------------------- */
+
+/* No counterpart in the reference (a batch benchmark).  A BFS server keeps
+ * several graphs resident on one GPU and answers (graph, root) queries as
+ * they arrive, with continuous batching: every graph has a few batch slots,
+ * each served by its own worker thread and CUDA stream; a free slot takes up
+ * to max_batch queued roots of its graph into one b200bfs_run_batch-style
+ * traversal, so requests that arrive while other batches are on the GPU are
+ * admitted as soon as a slot frees, and batches of different graphs (and of
+ * one graph on different slots) overlap on the device.  Graphs and slots are
+ * admitted against one HBM budget.  Each request's levels are those of a
+ * single-source search from its root, whatever batch it was served in.
+ * All server calls are thread-safe. */
+typedef struct b200bfs_server b200bfs_server;
+
+typedef struct b200bfs_server_config {
+  int device;                 /* CUDA device ordinal                          */
+  int max_batch;              /* roots per batch, 1..64 (0: 64)               */
+  int slots_per_graph;        /* concurrent batches per graph (0: 2)          */
+  int keep_results;           /* 1: a finished request keeps its levels on the
+                                 device until b200bfs_server_release          */
+  uint64_t hbm_budget_bytes;  /* graphs + slots together (0: device memory)   */
+  double alpha;               /* batch switch alpha (<= 0: 30)                */
+  double beta;                /* batch switch beta (<= 0: 14)                 */
+} b200bfs_server_config;
+
+enum {
+  B200BFS_REQ_QUEUED = 0,
+  B200BFS_REQ_RUNNING = 1,
+  B200BFS_REQ_DONE = 2,
+  B200BFS_REQ_FAILED = 3,
+  B200BFS_REQ_CANCELLED = 4
+};
+
+typedef struct b200bfs_request_info {
+  int32_t state;                 /* B200BFS_REQ_*                             */
+  int32_t graph_id;
+  int64_t root;
+  int32_t depth;                 /* deepest level reached from the root       */
+  int32_t batch_size;            /* roots in the batch that served it         */
+  double latency_ms;             /* submit -> done, host clock                */
+  double queue_ms;               /* submit -> start of its batch              */
+} b200bfs_request_info;
+
+typedef struct b200bfs_server_stats {
+  int64_t submitted;
+  int64_t completed;
+  int64_t failed;
+  int64_t batches;
+  double mean_batch_size;
+  double p50_ms;                 /* latency percentiles of completed requests */
+  double p99_ms;
+  double max_ms;
+  double bfs_per_s;              /* completed / (last completion - first submit) */
+  uint64_t device_bytes;         /* held by graphs and slots                  */
+  int32_t graphs;
+  int32_t slots;
+} b200bfs_server_stats;
+
+/* Starts a server (no graphs yet). */
+int b200bfs_server_start(const b200bfs_server_config* config, b200bfs_server** out);
+/* Generates and prepares a Graph500 graph on the device (as
+ * b200bfs_generate_graph + b200bfs_prepare with edgefactor's switch
+ * parameters) and makes it servable; B200BFS_ERR_OOM when it or its first
+ * slot does not fit the budget.  *graph_id receives its id. */
+int b200bfs_server_add_graph(b200bfs_server* srv, int scale, int edgefactor, uint64_t seed1,
+                             uint64_t seed2, int flags, int* graph_id);
+int b200bfs_server_graph_info(b200bfs_server* srv, int graph_id, b200bfs_graph_info* out);
+/* Queues a query; returns at once with its id. */
+int b200bfs_server_submit(b200bfs_server* srv, int graph_id, int64_t root, int64_t* request_id);
+/* State of a request, without waiting. */
+int b200bfs_server_poll(b200bfs_server* srv, int64_t request_id, b200bfs_request_info* info);
+/* Waits up to timeout_s seconds for a request to finish;
+ * B200BFS_ERR_TIMEOUT if it has not. */
+int b200bfs_server_wait(b200bfs_server* srv, int64_t request_id, double timeout_s,
+                        b200bfs_request_info* info);
+/* Levels of a finished request (keep_results = 1), levels[pred_size] in
+ * original vertex ids, -1 for unreached vertices. */
+int b200bfs_server_get_levels(b200bfs_server* srv, int64_t request_id, int32_t* levels);
+/* Forgets a request; a finished request's slot can then be reused. */
+int b200bfs_server_release(b200bfs_server* srv, int64_t request_id);
+int b200bfs_server_get_stats(b200bfs_server* srv, b200bfs_server_stats* out);
+/* Restarts the latency and throughput statistics. */
+int b200bfs_server_reset_stats(b200bfs_server* srv);
+const char* b200bfs_server_last_error(const b200bfs_server* srv);
+/* Stops the workers (queued requests are cancelled, running batches finish)
+ * and frees every graph. */
+int b200bfs_server_stop(b200bfs_server* srv);
+
 /* ------------------------- allocation-free search ------------------------ */
 
 /* Largest graph b200bfs_bfs_noalloc accepts (rows of the CSR). */

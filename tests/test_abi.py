@@ -55,3 +55,19 @@ def test_no_cpu_fallback_without_device(built):
         pytest.skip("a CUDA device is present")
     with pytest.raises(b200bfs.B200BfsError):
         b200bfs.Engine()
+
+
+def test_server_rejects_null_and_needs_a_device(built):
+    import ctypes
+    import torch
+    import b200bfs
+
+    L = b200bfs.load_library()
+    assert L.b200bfs_server_submit(None, 0, 0, None) == 1
+    assert L.b200bfs_server_stop(None) == 1
+    assert L.b200bfs_server_last_error(None) == b"null server"
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(b200bfs.B200BfsError) as ex:
+        b200bfs.Server(0)
+    assert ex.value.code == 2
