@@ -50,6 +50,10 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
                    help="alpha of the batched search (<= 0: the engine's batch default)")
+    p.add_argument("--serve-rates", default="1000,10000,100000",
+                   help="offered query rates (per s) of the serving leg")
+    p.add_argument("--serve-seconds", type=float, default=1.5)
+    p.add_argument("--no-serve", action="store_true")
     p.add_argument("--cpu-sample-sec", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -301,6 +305,62 @@ def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
     }
 
 
+# The serving workload: Kronecker graphs of the benchmark's generator resident
+# together, (SCALE, edgefactor).
+SERVE_GRAPHS = [(16, 16), (18, 16), (20, 16), (22, 16), (24, 16), (22, 8), (22, 32)]
+
+
+def serving_leg(args, device):
+    """BFS serving with continuous batching (b200bfs_server_*): the graphs of
+    SERVE_GRAPHS resident on the device under a 150 GB budget, (graph, root)
+    queries arriving as a Poisson process (graph uniform, root uniform over a
+    pool of 1024 vertices with edges per graph), for each offered rate.
+    Latency is submit -> result on the device, measured by the server."""
+    import b200bfs
+
+    srv = b200bfs.Server(device, keep_results=False, slots_per_graph=2,
+                         hbm_budget_bytes=150 * 10**9)
+    out = {"graphs": [f"SCALE {s} ef {ef}" for s, ef in SERVE_GRAPHS], "rates": []}
+    try:
+        t0 = time.time()
+        gids = [srv.add_graph(s, ef) for s, ef in SERVE_GRAPHS]
+        pools = [srv.find_roots(g, 1024) for g in gids]
+        out["build_s"] = time.time() - t0
+        for g, pool in zip(gids, pools):  # one batch per graph and slot builds the graphs
+            ids = [srv.submit(g, int(r)) for r in pool[:128]]
+            for rid in ids:
+                srv.wait(rid)
+                srv.release(rid)
+        rng = np.random.default_rng(12345)
+        for lam in [float(x) for x in args.serve_rates.split(",") if x]:
+            n = max(1, int(lam * args.serve_seconds))
+            t_arr = np.cumsum(rng.exponential(1.0 / lam, n))
+            gsel = rng.integers(0, len(gids), n)
+            rsel = rng.integers(0, 1024, n)
+            srv.reset_stats()
+            start = time.perf_counter()
+            for i in range(n):
+                while time.perf_counter() - start < t_arr[i]:
+                    pass
+                srv.submit(gids[gsel[i]], int(pools[gsel[i]][rsel[i]]))
+            t_sub = time.perf_counter() - start
+            deadline = time.perf_counter() + 120
+            while srv.stats().completed + srv.stats().failed < n and time.perf_counter() < deadline:
+                time.sleep(0.005)
+            st = srv.stats()
+            out["rates"].append({
+                "offered_per_s": lam, "submitted_per_s": n / t_sub, "requests": n,
+                "completed": st.completed, "failed": st.failed, "bfs_per_s": st.bfs_per_s,
+                "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
+                "mean_batch": st.mean_batch_size, "batches": st.batches})
+            log(f"serving at {lam:.0f}/s: {st.bfs_per_s:.0f} BFS/s, p50 {st.p50_ms:.2f} ms, "
+                f"p99 {st.p99_ms:.2f} ms, mean batch {st.mean_batch_size:.1f}")
+        out["device_bytes"] = srv.stats().device_bytes
+    finally:
+        srv.stop()
+    return out
+
+
 def workload_config(args):
     return {"workload": f"Graph500 Kronecker SCALE {args.scale} edgefactor {args.edgefactor} "
                         f"(A,B,C=.57,.19,.19, seeds 2/3), {args.roots} roots, single-source "
@@ -488,6 +548,8 @@ def main():
         del row_ptr, col, inv, mdeg
     eng.end()
     eng.close()
+    if world == 1 and not args.no_serve:
+        line["serving"] = serving_leg(args, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

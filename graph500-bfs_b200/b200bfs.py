@@ -41,6 +41,7 @@ SYMBOLS = [
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
     "b200bfs_validate", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
     "b200bfs_server_start", "b200bfs_server_add_graph", "b200bfs_server_graph_info",
+    "b200bfs_server_find_roots",
     "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
     "b200bfs_server_get_levels", "b200bfs_server_release", "b200bfs_server_get_stats",
     "b200bfs_server_reset_stats", "b200bfs_server_last_error", "b200bfs_server_stop",
@@ -175,6 +176,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_server_start.argtypes = [P(ServerConfig), P(S)]
     L.b200bfs_server_add_graph.argtypes = [S, i32, i32, u64, u64, i32, P(ctypes.c_int)]
     L.b200bfs_server_graph_info.argtypes = [S, i32, P(GraphInfo)]
+    L.b200bfs_server_find_roots.argtypes = [S, i32, i32, i32, i32, vp]
     L.b200bfs_server_submit.argtypes = [S, i32, i64, P(ctypes.c_int64)]
     L.b200bfs_server_poll.argtypes = [S, i64, P(RequestInfo)]
     L.b200bfs_server_wait.argtypes = [S, i64, dbl, P(RequestInfo)]
@@ -399,6 +401,11 @@ class Server:
         gi = GraphInfo()
         self.check(self.L.b200bfs_server_graph_info(self.s, gid, ctypes.byref(gi)))
         return gi
+
+    def find_roots(self, gid, num_roots, r1=0, r2=0):
+        out = np.zeros(num_roots, dtype=np.int64)
+        self.check(self.L.b200bfs_server_find_roots(self.s, gid, num_roots, r1, r2, _ptr(out)))
+        return out
 
     def submit(self, gid, root):
         rid = ctypes.c_int64()

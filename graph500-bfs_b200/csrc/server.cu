@@ -300,6 +300,20 @@ int b200bfs_server_graph_info(b200bfs_server* p, int graph_id, b200bfs_graph_inf
   });
 }
 
+int b200bfs_server_find_roots(b200bfs_server* p, int graph_id, int num_roots, int r1, int r2,
+                              int64_t* roots) {
+  return srv_guarded(p, [&](Server& s) {
+    b200bfs::GraphEntry* ge;
+    {
+      std::lock_guard<std::mutex> lk(s.mu);
+      ge = graph_of(s, graph_id);
+    }
+    std::lock_guard<std::mutex> dk(ge->decode_mu);
+    const int rc = b200bfs_find_roots(ge->h, num_roots, r1, r2, roots);
+    if (rc != B200BFS_OK) throw b200bfs::Error{rc, b200bfs_last_error(ge->h)};
+  });
+}
+
 int b200bfs_server_submit(b200bfs_server* p, int graph_id, int64_t root, int64_t* request_id) {
   return srv_guarded(p, [&](Server& s) {
     srv_require(request_id != nullptr, B200BFS_ERR_INVALID, "null output");

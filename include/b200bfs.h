@@ -360,6 +360,10 @@ int b200bfs_server_start(const b200bfs_server_config* config, b200bfs_server** o
 int b200bfs_server_add_graph(b200bfs_server* srv, int scale, int edgefactor, uint64_t seed1,
                              uint64_t seed2, int flags, int* graph_id);
 int b200bfs_server_graph_info(b200bfs_server* srv, int graph_id, b200bfs_graph_info* out);
+/* Roots of a served graph drawn as b200bfs_find_roots does (uniform among
+ * vertices with an edge), for load generators and tests. */
+int b200bfs_server_find_roots(b200bfs_server* srv, int graph_id, int num_roots, int r1, int r2,
+                              int64_t* roots);
 /* Queues a query; returns at once with its id. */
 int b200bfs_server_submit(b200bfs_server* srv, int graph_id, int64_t root, int64_t* request_id);
 /* State of a request, without waiting. */
