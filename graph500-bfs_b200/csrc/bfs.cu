@@ -417,6 +417,117 @@ __global__ void __launch_bounds__(256) td_wide_kernel(
   }
 }
 
+}  // namespace
+
+// Largest i in [lo, hi] with qdeg[i] <= t, given qdeg[lo] <= t; every lane
+// of the warp gets it.  Each step lets the 32 lanes probe 32 evenly spaced
+// entries, so a search over n entries takes log32(n) coalesced rounds.
+__device__ int64_t warp_segment_search(const int64_t* __restrict__ qdeg, int64_t lo, int64_t hi,
+                                       int64_t t) {
+  const int lane = lane_id();
+  while (hi - lo > 31) {
+    const int64_t step = (hi - lo + 31) / 32;
+    const int64_t probe = lo + step * lane;
+    const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
+    const int last = 31 - __clz(le);
+    const int64_t next = lo + step * (last + 1);  // first probe known to be > t
+    lo += step * last;
+    if (last < 31 && next <= hi) hi = next - 1;
+  }
+  const int64_t probe = lo + lane;
+  const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
+  return lo + (31 - __clz(le));
+}
+
+namespace {
+
+// Top-down expansion, third form.  Each warp takes a contiguous chunk of
+// kTdTile-entry tiles of the concatenated frontier rows and finds the row of
+// its first entry with one warp search; from there it steps 32 entries at a
+// time, carrying the current row.  When all 32 entries of a step lie in the
+// current row (the hub rows of the large levels) they need no lookup at all;
+// otherwise the rows starting inside the step (at most 31, since every row
+// has an edge) mark their start positions in a 32-slot array and a
+// prefix-max over the lanes gives each entry its row, so frontiers of many
+// short rows (the tail levels) do not walk the degree prefix row by row.
+__global__ void __launch_bounds__(256) td_chunk_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  __shared__ int s_map[8][32];
+  const int64_t qsize = (int64_t)ctr->qsize;
+  if (qsize == 0) return;
+  const int64_t total = qdeg[qsize];
+  const int lane = lane_id();
+  const int w = threadIdx.x >> 5;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (total + kTdTile - 1) / kTdTile;
+  const int64_t per = (ntiles + nwarps - 1) / nwarps;
+  const int64_t e_begin = gw * per * kTdTile;
+  const int64_t e_end = min(total, (gw + 1) * per * kTdTile);
+  if (e_begin >= e_end) return;
+  int64_t base = warp_segment_search(qdeg, 0, qsize - 1, e_begin);
+  int64_t b_lo = qdeg[base], b_hi = qdeg[base + 1];
+  int32_t b_src = queue[base];
+  int64_t b_rb = row_ptr[b_src];
+  for (int64_t e0 = e_begin; e0 < e_end; e0 += 32) {
+    const int64_t e = e0 + lane;
+    const int64_t last = min(e0 + 31, e_end - 1);
+    int32_t src = b_src;
+    int64_t lo = b_lo, rb = b_rb, seg_last = base;
+    if (last >= b_hi) {
+      s_map[w][lane] = 0;
+      __syncwarp();
+      const int64_t j = base + 1 + lane;
+      if (j < qsize) {
+        const int64_t p = qdeg[j] - e0;
+        if (p >= 0 && p < 32) s_map[w][p] = lane + 1;
+      }
+      __syncwarp();
+      int off = s_map[w][lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, off, o);
+        if (lane >= o) off = max(off, t);
+      }
+      const int64_t seg = base + off;
+      if (off) {
+        src = queue[seg];
+        lo = qdeg[seg];
+        rb = row_ptr[src];
+      }
+      seg_last = __shfl_sync(kFull, seg, 31);
+      __syncwarp();
+    }
+    if (e < e_end) {
+      const int32_t u = __ldg(col + rb + (e - lo));
+      const uint32_t bit = 1u << (u & 31);
+      if ((vis[u >> 5] & bit) == 0) {
+        pred[__ldg(inv + u)] = pred_entry(__ldg(inv + src), level);
+        red_or(vis + (u >> 5), bit);
+      }
+    }
+    // row of entry e0 + 32: the row of the step's last entry, or the next one
+    // when that row ends exactly there
+    if (seg_last != base) {
+      base = seg_last;
+      b_lo = qdeg[base];
+      b_hi = qdeg[base + 1];
+      b_src = queue[base];
+      b_rb = row_ptr[b_src];
+    }
+    if (b_hi <= e0 + 32 && base + 1 < qsize) {
+      ++base;
+      b_lo = b_hi;
+      b_hi = qdeg[base + 1];
+      b_src = queue[base];
+      b_rb = row_ptr[b_src];
+    }
+  }
+}
+
 // Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
 // vertices, their CSR degrees and their pre-dedup degrees.
 __global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
@@ -658,6 +769,14 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   const int td_grid = sms * 8;
   const int bu_grid = grid_for(st.W * 32, B, sms, 8);
   const int bu_wide_grid = sms * 8;
+  // the chunked top-down form splits the work evenly over its warps, so its
+  // grid is exactly the resident blocks (one wave)
+  static int chunk_per_sm = 0;
+  if (!chunk_per_sm &&
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&chunk_per_sm, td_chunk_kernel, B, 0) !=
+          cudaSuccess)
+    chunk_per_sm = 4;
+  const int td_chunk_grid = sms * std::max(chunk_per_sm, 1);
   for (;;) {
     ++level;
     if (level > kMaxLevel) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
@@ -672,9 +791,16 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     nev += 2;
     if (forward) {
       ++rs.num_td_levels;
-      if (opt.td_kernel == 1)
+      // form 4: the strided form while the frontier grows (hub rows), the
+      // chunked form once the search has come back from bottom-up (short
+      // rows of the tail levels)
+      const int td_form = opt.td_kernel == 4 ? (growing ? 1 : 3) : opt.td_kernel;
+      if (td_form == 1)
         td_expand_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
                                                st.vis[cur], st.pred, level);
+      else if (td_form == 3)
+        td_chunk_kernel<<<td_chunk_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,
+                                                    c.inv, st.vis[cur], st.pred, level);
       else
         td_wide_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
                                              st.vis[cur], st.pred, level);

@@ -524,7 +524,7 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
       require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "bu_kernel must be 1..4");
       e.opt.bu_kernel = (int)value;
     } else if (n == "td_kernel") {
-      require(value >= 1 && value <= 2, B200BFS_ERR_INVALID, "td_kernel must be 1..2");
+      require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "td_kernel must be 1..4");
       e.opt.td_kernel = (int)value;
     } else if (n == "bu_probe") {
       require(value >= 1 && value <= 64, B200BFS_ERR_INVALID, "bu_probe must be 1..64");

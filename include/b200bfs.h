@@ -243,7 +243,7 @@ int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
 
 /* Engine tuning knobs (no counterpart in the reference, whose equivalents
  * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
- * kernel form), "td_kernel" (1..2, top-down kernel form), "bu_probe" (1..64,
+ * kernel form), "td_kernel" (1..4, top-down kernel form; 4 picks per level), "bu_probe" (1..64,
  * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
  * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2),
  * "batch_graph" (1: b200bfs_run_batch runs its level loop as a CUDA graph on

@@ -236,7 +236,7 @@ def test_hbm_budget_admission(built):
     e.close()
 
 
-@pytest.mark.parametrize("bu,td", [(1, 1), (2, 2), (3, 1), (4, 2)])
+@pytest.mark.parametrize("bu,td", [(1, 1), (2, 2), (3, 1), (4, 2), (4, 3), (4, 4)])
 def test_kernel_forms_agree(engine, oracle_graphs, bu, td):
     """Every bottom-up / top-down kernel form gives the reference levels."""
     edges, g = oracle_graphs(18)
@@ -248,6 +248,6 @@ def test_kernel_forms_agree(engine, oracle_graphs, bu, td):
         _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 3))
         _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 2), alpha=1e-9)
     finally:
-        engine.set_option("bu_kernel", 2)
-        engine.set_option("td_kernel", 2)
+        engine.set_option("bu_kernel", 4)
+        engine.set_option("td_kernel", 4)
         engine.end()
