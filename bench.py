@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
                    help="alpha of the batched search (<= 0: the engine's batch default)")
+    p.add_argument("--batch-host-loop", action="store_true",
+                   help="batched search with the host-driven level loop (for profilers that "
+                        "cannot see kernels inside conditional CUDA graphs)")
     p.add_argument("--serve-rates", default="1000,10000,100000",
                    help="offered query rates (per s) of the serving leg")
     p.add_argument("--serve-seconds", type=float, default=1.5)
@@ -263,6 +266,8 @@ def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
     import torch
 
     k = min(args.batch_roots, len(roots), 64)
+    if args.batch_host_loop:
+        eng.set_option("batch_graph", 0)
     for w in range(max(args.warmup, 3)):
         eng.run_batch(np.roll(roots, w)[:k], args.edgefactor, args.batch_alpha, args.beta)
     times, stats = [], None
