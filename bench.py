@@ -44,8 +44,14 @@ def parse():
     p.add_argument("--root-seed", type=int, default=0)
     p.add_argument("--alpha", type=float, default=10.0)
     p.add_argument("--beta", type=float, default=14.0)
-    p.add_argument("--corebfs", action="store_true")
-    p.add_argument("--group-reorder", action="store_true")
+    # The SCALE 28 workload runs as the reference's -A -C with degree-ordered
+    # group reordering; each part can be switched off.
+    p.add_argument("--no-corebfs", dest="corebfs", action="store_false",
+                   help="without CoreBFS forest pruning (-C)")
+    p.add_argument("--no-group-reorder", dest="group_reorder", action="store_false",
+                   help="one global degree order instead of groups of 2^16 ids")
+    p.add_argument("--no-auto-tune", dest="auto_tune", action="store_false",
+                   help="without the -A alpha/beta tuner")
     p.add_argument("--batch-roots", type=int, default=64)
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
@@ -254,6 +260,29 @@ def rows_of(inv, roots, nverts):
     return rank[np.asarray(roots, dtype=np.int64)]
 
 
+def cpu_baseline_leg(args, device, roots, nedge):
+    """The reference's plain CPU search (no -A, no -C: the default
+    `mpiexec -n 1 runnable` run), restated by the oracle, timed on all host
+    cores over a bounded sample of the same roots on the same generated graph
+    (built on the device without pruning and copied to host memory)."""
+    import b200bfs
+
+    eng = b200bfs.Engine(device)
+    eng.generate_graph(args.scale, args.edgefactor)
+    info = eng.info()
+    row_ptr, col, inv, mdeg = host_csr(eng)
+    eng.close()
+    rows = rows_of(inv, roots, 1 << info.scale)
+    plain = argparse.Namespace(**vars(args))
+    plain.alpha, plain.beta = 10.0, 14.0
+    ct, cu, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size, rows, nedge,
+                                      plain, args.cpu_sample_sec)
+    return {"value": harmonic_teps(cu, ct) / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
+            "sample": f"{len(ct)} searches at SCALE {args.scale} (about {sum(ct):.0f} s) with the "
+                      "oracle's OpenMP restatement of BfsBase::run_bfs_core (plain, alpha 10, "
+                      "beta 14) on the same graph and roots"}
+
+
 def percentile(x, q):
     return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
 
@@ -367,9 +396,12 @@ def serving_leg(args, device):
 
 
 def workload_config(args):
+    mode = " ".join(x for x, on in (("-A", args.auto_tune), ("-C", args.corebfs),
+                                    ("group reordering", args.group_reorder)) if on) or "plain"
     return {"workload": f"Graph500 Kronecker SCALE {args.scale} edgefactor {args.edgefactor} "
                         f"(A,B,C=.57,.19,.19, seeds 2/3), {args.roots} roots, single-source "
-                        "direction-optimizing BFS",
+                        f"direction-optimizing BFS, {mode}",
+            "auto_tune": bool(args.auto_tune),
             "scale": args.scale, "edgefactor": args.edgefactor, "roots": args.roots,
             "corebfs": bool(args.corebfs), "group_reorder": bool(args.group_reorder),
             "alpha": args.alpha, "beta": args.beta,
@@ -387,7 +419,9 @@ def run_reference(args, rank, world, dist):
 
     t0 = time.time()
     eng = b200bfs.Engine(0)
-    eng.generate_graph(args.scale, args.edgefactor, flags=build_flags(args))
+    # the reference's plain CPU run (no -A, no -C) on the same generated graph
+    args.alpha, args.beta = 10.0, 14.0
+    eng.generate_graph(args.scale, args.edgefactor)
     eng.prepare(args.edgefactor, args.alpha, args.beta)
     roots, nedge = pick_roots(eng, args)
     info = eng.info()
@@ -447,6 +481,12 @@ def main():
         f"{info.device_bytes / 1e9:.1f} GB on device")
     roots, nedge = pick_roots(eng, args)
     log(f"[rank {rank}] roots validated; nedge {int(nedge.min())}..{int(nedge.max())}")
+    if args.auto_tune:
+        t0 = time.time()
+        args.alpha, args.beta, _ = eng.auto_tune(roots, nedge, args.edgefactor, args.alpha,
+                                                 args.beta)
+        log(f"[rank {rank}] -A tuning: alpha {args.alpha:.4g}, beta {args.beta:.4g} "
+            f"({time.time() - t0:.1f}s)")
 
     stream = torch.cuda.ExternalStream(eng.stream())
     order = [i % len(roots) for i in range(args.warmup + args.steps)]
@@ -541,18 +581,10 @@ def main():
                    "td_ms": td_ms / args.steps, "bu_ms": bu_ms / args.steps,
                    "build_s": t_build},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        row_ptr, col, inv, mdeg = host_csr(eng)
-        rows = rows_of(inv, roots, 1 << info.scale)
-        ct, cu, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size, rows, nedge,
-                                          args, args.cpu_sample_sec)
-        line["cpu_baseline"] = {
-            "value": harmonic_teps(cu, ct) / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
-            "sample": f"{len(ct)} searches at SCALE {args.scale} (about {sum(ct):.0f} s) with the "
-                      "oracle's OpenMP restatement of BfsBase::run_bfs_core on the same graph"}
-        del row_ptr, col, inv, mdeg
     eng.end()
     eng.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_leg(args, local, roots, nedge)
     if world == 1 and not args.no_serve:
         line["serving"] = serving_leg(args, local)
     if rank == 0:

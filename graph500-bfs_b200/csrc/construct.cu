@@ -12,7 +12,12 @@
 //      taken within groups of 2^16 original ids, SMALL_REORDER_BIT :594-732);
 //   4. place every directed entry into its row (two-pass counting placement),
 //      sort each row and drop duplicates (sortEdgesInner, :1986-2056) to get
-//      num_global_edges_ (:2100) and num_global_verts_ (:2103-2128).
+//      num_global_edges_ (:2100) and num_global_verts_ (:2103-2128).  Rows
+//      are sorted by the neighbours' global degree rank (highest degree
+//      first) even with group reordering, where the reference sorts by the
+//      group-ordered id: adjacency order changes neither levels nor the
+//      validity of parents, and hub-first lists let the bottom-up searches
+//      stop early.
 // Self-loops are dropped as in make_symmetry_edge_list (:409, 429, 447).
 // All passes are bandwidth-bound integer streams; CUB supplies the radix
 // sorts and scans of this (untimed) construction step.
@@ -78,8 +83,11 @@ __global__ void rank_kernel(const int32_t* __restrict__ inv, const uint32_t* __r
   }
 }
 
+// Places every edge in its source row; the stored value is the neighbour's
+// sort key nkey[v] (its row id, or its global degree rank when rows follow
+// the group order).
 __global__ void scatter_kernel(const uint2* __restrict__ e, int64_t m, bool mirror,
-                               const int32_t* __restrict__ rank,
+                               const int32_t* __restrict__ rank, const int32_t* __restrict__ nkey,
                                const int64_t* __restrict__ raw_ptr,
                                uint32_t* __restrict__ cursor, int32_t* __restrict__ raw) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
@@ -87,8 +95,21 @@ __global__ void scatter_kernel(const uint2* __restrict__ e, int64_t m, bool mirr
     uint2 x = e[i];
     if (x.x == x.y) continue;
     int32_t ra = rank[x.x], rb = rank[x.y];
-    raw[raw_ptr[ra] + atomicAdd(cursor + ra, 1u)] = rb;
-    if (mirror) raw[raw_ptr[rb] + atomicAdd(cursor + rb, 1u)] = ra;
+    raw[raw_ptr[ra] + atomicAdd(cursor + ra, 1u)] = nkey[x.y];
+    if (mirror) raw[raw_ptr[rb] + atomicAdd(cursor + rb, 1u)] = nkey[x.x];
+  }
+}
+
+// Group order: nkey[v] = position of v in the global degree order,
+// row_of_key[k] = row of the vertex at global position k.
+__global__ void global_rank_kernel(const int32_t* __restrict__ gorder, int64_t R,
+                                   const int32_t* __restrict__ rank, int32_t* __restrict__ nkey,
+                                   int32_t* __restrict__ row_of_key) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < R;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = gorder[k];
+    nkey[v] = (int32_t)k;
+    row_of_key[k] = rank[v];
   }
 }
 
@@ -134,6 +155,7 @@ __global__ void count_distinct_kernel(const int32_t* __restrict__ raw,
 __global__ void compact_rows_kernel(const int32_t* __restrict__ raw,
                                     const int64_t* __restrict__ raw_ptr, int64_t R,
                                     const int64_t* __restrict__ row_ptr,
+                                    const int32_t* __restrict__ row_of_key,
                                     int32_t* __restrict__ col) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -149,7 +171,7 @@ __global__ void compact_rows_kernel(const int32_t* __restrict__ raw,
         head = (j == b) || (x != raw[j - 1]);
       }
       unsigned m = __ballot_sync(kFull, head);
-      if (head) col[out + __popc(m & ((1u << lane) - 1))] = x;
+      if (head) col[out + __popc(m & ((1u << lane) - 1))] = row_of_key ? row_of_key[x] : x;
       out += __popc(m);
     }
   }
@@ -248,6 +270,34 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   int64_t* raw_ptr = arena_alloc<int64_t>(arena, R + 1, "raw row ptr");
   int64_t* len64 = arena_alloc<int64_t>(arena, R, "row len");
   rank_kernel<<<grid(R), B, 0, s>>>(c.inv, deg, R, c.rank, c.mdeg, len64);
+  // Neighbour lists are sorted by the neighbours' global degree rank, highest
+  // degree first, whatever the row numbering: the bottom-up searches stop at
+  // the first neighbour found, and the hubs are found first.  With one global
+  // degree order the rank is the row id; with the group order it comes from a
+  // second sort by degree alone.
+  int32_t* nkey = c.rank;
+  int32_t* row_of_key = nullptr;
+  if (group_bits > 0) {
+    uint64_t* k1 = arena_alloc<uint64_t>(arena, n, "sort keys");
+    uint64_t* k2 = arena_alloc<uint64_t>(arena, n, "sort keys");
+    int32_t* i1 = arena_alloc<int32_t>(arena, n, "sort values");
+    int32_t* i2 = arena_alloc<int32_t>(arena, n, "sort values");
+    make_keys_kernel<<<grid(n), B, 0, s>>>(deg, n, 0, k1, i1);
+    size_t tmp = 0;
+    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k1, k2, i1, i2, (int)n, 0, 64, s),
+               "sort size");
+    void* t = arena.alloc(tmp, "sort temp");
+    check_cuda(cub::DeviceRadixSort::SortPairs(t, tmp, k1, k2, i1, i2, (int)n, 0, 64, s),
+               "sort");
+    arena.free(t);
+    arena.free(k1);
+    arena.free(k2);
+    arena.free(i1);
+    nkey = arena_alloc<int32_t>(arena, n, "neighbour keys");
+    row_of_key = arena_alloc<int32_t>(arena, R, "key to row");
+    global_rank_kernel<<<grid(R), B, 0, s>>>(i2, R, c.rank, nkey, row_of_key);
+    arena.free(i2);
+  }
   arena.free(deg);
   check_cuda(cudaMemsetAsync(raw_ptr, 0, 8, s), "memset");
   {
@@ -266,7 +316,8 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   int32_t* raw = arena_alloc<int32_t>(arena, total, "raw adjacency");
   uint32_t* cursor = arena_alloc<uint32_t>(arena, R, "cursor");
   check_cuda(cudaMemsetAsync(cursor, 0, R * 4, s), "memset");
-  scatter_kernel<<<grid(m), B, 0, s>>>(edges, m, mirror, c.rank, raw_ptr, cursor, raw);
+  scatter_kernel<<<grid(m), B, 0, s>>>(edges, m, mirror, c.rank, nkey, raw_ptr, cursor, raw);
+  if (nkey != c.rank) arena.free(nkey);
   arena.free(cursor);
 
   // 5. per-row sort in chunks of at most 2^30 entries
@@ -336,7 +387,7 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   check_cuda(cudaMemcpyAsync(&c.nedges, c.row_ptr + R, 8, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "dedup count");
   c.col = arena_alloc<int32_t>(arena, c.nedges, "adjacency");
-  compact_rows_kernel<<<grid(R * 32), B, 0, s>>>(raw, raw_ptr, R, c.row_ptr, c.col);
+  compact_rows_kernel<<<grid(R * 32), B, 0, s>>>(raw, raw_ptr, R, c.row_ptr, row_of_key, c.col);
   check_cuda(cudaMemsetAsync(d_u64, 0, 8, s), "memset");
   max_degree_kernel<<<grid(R), B, 0, s>>>(c.row_ptr, R, d_u64);
   unsigned long long maxd = 0;
@@ -347,6 +398,7 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   arena.free(raw_ptr);
   arena.free(len64);
   arena.free(d_u64);
+  if (row_of_key) arena.free(row_of_key);
   check_cuda(cudaGetLastError(), "build_csr");
 }
 

@@ -72,10 +72,12 @@ T* arena_alloc(DeviceArena& a, int64_t n, const char* what) {
 
 void check_cuda(cudaError_t e, const char* what);  // throws Error on failure
 
-// A CSR over reordered vertex ids ("rows").  Row r holds the sorted,
-// de-duplicated neighbours of original vertex inv[r]; rows are in descending
-// order of the pre-dedup degree (optionally within groups of 2^reorder_bits
-// original ids), so low row ids are the high-degree vertices.
+// A CSR over reordered vertex ids ("rows").  Row r holds the de-duplicated
+// neighbours of original vertex inv[r], highest pre-dedup degree first; rows
+// are in descending order of the pre-dedup degree (optionally within groups
+// of 2^reorder_bits original ids, when the neighbour order is the global
+// degree order rather than the row order), so without groups low row ids
+// are the high-degree vertices and neighbour lists are ascending.
 struct Csr {
   int64_t nrows = 0;           // R: vertices with >= 1 edge
   int64_t nedges = 0;          // E: directed entries after de-duplication

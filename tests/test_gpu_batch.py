@@ -123,6 +123,17 @@ def test_batch_corebfs(engine, graphs, scale):
     _check_batch(engine, edges, g, roots, corebfs=True)
 
 
+def test_batch_group_reorder_corebfs(engine, graphs):
+    import b200bfs
+
+    edges, g = graphs(16)
+    core = O.Core(g)
+    engine.generate_graph(16, 16, flags=b200bfs.BUILD_COREBFS | b200bfs.BUILD_GROUP_REORDER)
+    engine.prepare(16)
+    roots = O.find_roots(core.has_edge(), 1 << 16, 64, 2)
+    _check_batch(engine, edges, g, roots, corebfs=True)
+
+
 def test_batch_long_path_grows_planes(engine):
     """A 60-vertex path has 60 levels: more than the 16 level planes a batch
     starts with, so the plane pool must grow during the search."""

@@ -165,6 +165,14 @@ def test_group_reorder(engine, oracle_graphs):
     assert (gi.num_global_edges, gi.num_global_verts) == (g.num_edges, g.num_verts)
     engine.prepare(16)
     _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 4))
+    # neighbour lists: the oracle's neighbour sets, highest degree first
+    row_ptr, col, inv, mdeg = engine.get_csr()
+    rng = np.random.default_rng(3)
+    for r in rng.integers(0, len(inv), 200):
+        nb = col[row_ptr[r]:row_ptr[r + 1]]
+        assert np.all(np.diff(mdeg[nb]) <= 0)
+        v = int(inv[r])
+        assert np.array_equal(np.sort(inv[nb]), g.col[g.row_ptr[v]:g.row_ptr[v + 1]])
     engine.end()
 
 
