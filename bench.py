@@ -52,6 +52,8 @@ def parse():
                    help="one global degree order instead of groups of 2^16 ids")
     p.add_argument("--no-auto-tune", dest="auto_tune", action="store_false",
                    help="without the -A alpha/beta tuner")
+    p.add_argument("--no-tune-engine", dest="tune_engine", action="store_false",
+                   help="keep the default kernel forms and batch alpha instead of timing them")
     p.add_argument("--batch-roots", type=int, default=64)
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
@@ -487,6 +489,11 @@ def main():
                                                  args.beta)
         log(f"[rank {rank}] -A tuning: alpha {args.alpha:.4g}, beta {args.beta:.4g} "
             f"({time.time() - t0:.1f}s)")
+    tuner = None
+    if args.tune_engine:
+        t0 = time.time()
+        tuner = eng.tune_engine(roots, args.edgefactor, args.alpha, args.beta).as_dict()
+        log(f"[rank {rank}] engine tuner: {tuner} ({time.time() - t0:.1f}s)")
 
     stream = torch.cuda.ExternalStream(eng.stream())
     order = [i % len(roots) for i in range(args.warmup + args.steps)]
@@ -574,6 +581,7 @@ def main():
         "clocks": clk,
         "gpu_launches": int(barrier_sum(dist, sum(s.kernel_launches for s in stats))),
         "batched": batched,
+        "engine_tuner": tuner,
         "search": {"edges_scanned_per_input_edge":
                        float(np.mean([(s.edges_scanned_td + s.edges_scanned_bu) for s in stats]))
                        / (info.num_input_edges or 1),

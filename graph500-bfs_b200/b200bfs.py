@@ -41,7 +41,7 @@ SYMBOLS = [
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
     "b200bfs_validate", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
     "b200bfs_server_start", "b200bfs_server_add_graph", "b200bfs_server_graph_info",
-    "b200bfs_server_find_roots",
+    "b200bfs_server_find_roots", "b200bfs_tune_engine",
     "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
     "b200bfs_server_get_levels", "b200bfs_server_release", "b200bfs_server_get_stats",
     "b200bfs_server_reset_stats", "b200bfs_server_last_error", "b200bfs_server_stop",
@@ -102,6 +102,19 @@ class BatchStats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+TUNE_FORMS, TUNE_BATCH_ALPHA = 1, 2
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("bu_kernel", ctypes.c_int32), ("td_kernel", ctypes.c_int32),
+                ("batch_alpha", ctypes.c_double), ("single_ms", ctypes.c_double),
+                ("batch_ms", ctypes.c_double), ("searches", ctypes.c_int32),
+                ("batches", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ServerConfig(ctypes.Structure):
@@ -171,6 +184,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
     L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
+    L.b200bfs_tune_engine.argtypes = [H, vp, i32, i32, dbl, dbl, i32, P(TuneReport)]
     L.b200bfs_batch_select.argtypes = [H, i32]
     S = ctypes.c_void_p
     L.b200bfs_server_start.argtypes = [P(ServerConfig), P(S)]
@@ -341,6 +355,15 @@ class Engine:
         self.check(self.L.b200bfs_run_batch(self.h, _ptr(r), len(r), edgefactor, alpha, beta,
                                             ctypes.byref(bs)))
         return bs
+
+    def tune_engine(self, roots, edgefactor=16, alpha=DEFAULT_ALPHA, beta=DEFAULT_BETA,
+                    what=TUNE_FORMS | TUNE_BATCH_ALPHA):
+        """Engine autotuner (b200bfs_tune_engine); returns the TuneReport."""
+        r = np.ascontiguousarray(np.asarray(roots, dtype=np.int64))
+        rep = TuneReport()
+        self.check(self.L.b200bfs_tune_engine(self.h, _ptr(r), len(r), edgefactor, alpha, beta,
+                                              what, ctypes.byref(rep)))
+        return rep
 
     def batch_select(self, index):
         """Makes root `index` of the last batch the current result (pred,

@@ -87,6 +87,9 @@ __global__ void root_kernel(int64_t root, const int32_t* __restrict__ rank,
 
 // Edge-balanced top-down expansion.  Frontier queue[0..qsize) with
 // qdeg[i] = sum of degrees of queue[0..i) (qdeg[qsize] = total).
+// kWarpSearch: the tile's first row is found by a 32-way warp search
+// (log32 rounds of coalesced loads) instead of lane 0's binary search.
+template <bool kWarpSearch>
 __global__ void __launch_bounds__(256) td_expand_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -101,17 +104,22 @@ __global__ void __launch_bounds__(256) td_expand_kernel(
   const int64_t ntiles = (total + kTdTile - 1) / kTdTile;
   for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
     const int64_t t0 = tile * kTdTile;
-    int64_t i0 = 0;
-    if (lane == 0) {
-      int64_t lo = 0, hi = qsize - 1;  // largest i with qdeg[i] <= t0
-      while (lo < hi) {
-        int64_t mid = (lo + hi + 1) >> 1;
-        if (qdeg[mid] <= t0) lo = mid;
-        else hi = mid - 1;
+    int64_t i;
+    if (kWarpSearch) {
+      i = warp_segment_search(qdeg, 0, qsize - 1, t0);
+    } else {
+      int64_t i0 = 0;
+      if (lane == 0) {
+        int64_t lo = 0, hi = qsize - 1;  // largest i with qdeg[i] <= t0
+        while (lo < hi) {
+          int64_t mid = (lo + hi + 1) >> 1;
+          if (qdeg[mid] <= t0) lo = mid;
+          else hi = mid - 1;
+        }
+        i0 = lo;
       }
-      i0 = lo;
+      i = __shfl_sync(kFull, i0, 0);
     }
-    int64_t i = __shfl_sync(kFull, i0, 0);
     int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
     int32_t src = queue[i];
     int64_t rbeg = row_ptr[src];
@@ -416,30 +424,6 @@ __global__ void __launch_bounds__(256) td_wide_kernel(
     }
   }
 }
-
-}  // namespace
-
-// Largest i in [lo, hi] with qdeg[i] <= t, given qdeg[lo] <= t; every lane
-// of the warp gets it.  Each step lets the 32 lanes probe 32 evenly spaced
-// entries, so a search over n entries takes log32(n) coalesced rounds.
-__device__ int64_t warp_segment_search(const int64_t* __restrict__ qdeg, int64_t lo, int64_t hi,
-                                       int64_t t) {
-  const int lane = lane_id();
-  while (hi - lo > 31) {
-    const int64_t step = (hi - lo + 31) / 32;
-    const int64_t probe = lo + step * lane;
-    const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
-    const int last = 31 - __clz(le);
-    const int64_t next = lo + step * (last + 1);  // first probe known to be > t
-    lo += step * last;
-    if (last < 31 && next <= hi) hi = next - 1;
-  }
-  const int64_t probe = lo + lane;
-  const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
-  return lo + (31 - __clz(le));
-}
-
-namespace {
 
 // Top-down expansion, third form.  Each warp takes a contiguous chunk of
 // kTdTile-entry tiles of the concatenated frontier rows and finds the row of
@@ -794,9 +778,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // form 4: the strided form while the frontier grows (hub rows), the
       // chunked form once the search has come back from bottom-up (short
       // rows of the tail levels)
-      const int td_form = opt.td_kernel == 4 ? (growing ? 1 : 3) : opt.td_kernel;
-      if (td_form == 1)
-        td_expand_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
+      const int td_form = opt.td_kernel == 4 ? (growing ? 5 : 3) : opt.td_kernel;
+      if (td_form == 5)
+        td_expand_kernel<true><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,
+                                                     c.inv, st.vis[cur], st.pred, level);
+      else if (td_form == 1)
+        td_expand_kernel<false><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
                                                st.vis[cur], st.pred, level);
       else if (td_form == 3)
         td_chunk_kernel<<<td_chunk_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,

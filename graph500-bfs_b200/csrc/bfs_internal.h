@@ -43,8 +43,9 @@ struct RunOptions {
   // at 4 per SM.  Form 4 is the fastest measured at SCALE 24 and 28.
   int bu_kernel = 4;
   // Top-down form.  1: td_expand_kernel, 2: td_wide_kernel, 3: td_chunk_kernel,
-  // 4: form 1 while the frontier grows, form 3 after the switch back from
-  // bottom-up (measured best at SCALE 24 and 28).
+  // 4: form 5 while the frontier grows, form 3 after the switch back from
+  // bottom-up (measured best at SCALE 24 and 28), 5: td_expand_kernel with a
+  // warp-wide search for each tile's first row.
   int td_kernel = 4;
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1

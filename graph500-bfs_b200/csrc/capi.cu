@@ -524,7 +524,7 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
       require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "bu_kernel must be 1..4");
       e.opt.bu_kernel = (int)value;
     } else if (n == "td_kernel") {
-      require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "td_kernel must be 1..4");
+      require(value >= 1 && value <= 5, B200BFS_ERR_INVALID, "td_kernel must be 1..5");
       e.opt.td_kernel = (int)value;
     } else if (n == "bu_probe") {
       require(value >= 1 && value <= 64, B200BFS_ERR_INVALID, "bu_probe must be 1..64");
@@ -587,6 +587,7 @@ int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, in
     for (int i = 0; i < num_roots; ++i)
       require(roots[i] >= 0 && roots[i] < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
     b200bfs_batch_stats rs;
+    b200bfs::ensure_batch_view(e.arena, e.g, e.stream, e.sms);
     b200bfs::run_batch(e.arena, e.g, e.bs, e.stream, e.sms, roots, num_roots, edgefactor,
                        alpha > 0 ? alpha : e.opt.batch_alpha, beta, e.opt.batch_graph != 0, &rs);
     e.st.levels = e.bs.level_records;

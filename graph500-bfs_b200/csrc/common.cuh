@@ -28,6 +28,26 @@ __device__ __forceinline__ void red_or(uint32_t* p, uint32_t v) { atomicOr(p, v)
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// Largest i in [lo, hi] with qdeg[i] <= t, given qdeg[lo] <= t; every lane
+// of the warp gets it.  Each step lets the 32 lanes probe 32 evenly spaced
+// entries, so a search over n entries takes log32(n) coalesced rounds.
+__device__ __forceinline__ int64_t warp_segment_search(const int64_t* __restrict__ qdeg,
+                                                       int64_t lo, int64_t hi, int64_t t) {
+  const int lane = lane_id();
+  while (hi - lo > 31) {
+    const int64_t step = (hi - lo + 31) / 32;
+    const int64_t probe = lo + step * lane;
+    const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
+    const int last = 31 - __clz(le);
+    const int64_t next = lo + step * (last + 1);  // first probe known to be > t
+    lo += step * last;
+    if (last < 31 && next <= hi) hi = next - 1;
+  }
+  const int64_t probe = lo + lane;
+  const unsigned le = __ballot_sync(kFull, probe <= hi && qdeg[probe] <= t);
+  return lo + (31 - __clz(le));
+}
+
 // Grid size helper: a multiple of the SM count times resident blocks.
 inline int grid_for(int64_t work_items, int block, int sms, int per_sm = 8) {
   int64_t need = (work_items + block - 1) / block;

@@ -111,6 +111,11 @@ struct Graph {
   Csr csr;                     // the searched graph (the 2-core with CoreBFS)
   CoreIndex core;
   uint2* input_edges = nullptr;  // device copy of the input edges, for validation
+  // The searched graph renumbered in global degree order, for the batched
+  // search on group-reordered graphs (built on first use; csr otherwise).
+  Csr bview;
+  int32_t* b_of_row = nullptr;   // [csr.nrows] row -> bview row
+  bool bview_built = false;
   bool input_symmetric = false;
   int64_t device_bytes = 0;
 };

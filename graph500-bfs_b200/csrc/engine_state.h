@@ -29,6 +29,7 @@ struct Engine {
     bs.release(arena);
     prepared = false;
     have_run = false;
+    free_batch_view(arena, g);
     free_core(arena, g);
     arena.free(g.csr.row_ptr);
     arena.free(g.csr.col);

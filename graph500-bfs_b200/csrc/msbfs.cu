@@ -21,6 +21,7 @@
 // reads back whether to continue.
 #include <algorithm>
 #include <cstring>
+#include <cub/cub.cuh>
 #include "common.cuh"
 #include "corebfs.h"
 #include "msbfs.h"
@@ -262,17 +263,7 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
   unsigned long long found = 0;
   for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
     const int64_t t0 = tile * kBTile;
-    int64_t i0 = 0;
-    if (lane == 0) {
-      int64_t lo = 0, hi = qsize - 1;  // largest i with qdeg[i] <= t0
-      while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if (qdeg[mid] <= t0) lo = mid;
-        else hi = mid - 1;
-      }
-      i0 = lo;
-    }
-    int64_t i = __shfl_sync(kFull, i0, 0);
+    int64_t i = warp_segment_search(qdeg, 0, qsize - 1, t0);
     int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
     int32_t src = queue[i];
     int64_t rbeg = row_ptr[src];
@@ -579,12 +570,15 @@ __global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
 
 // Initialises the control block for a new batch (64 threads).
 __global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, const BatchSetupArg* __restrict__ ap,
-                                   const int32_t* __restrict__ rank, int64_t nverts) {
+                                   const int32_t* __restrict__ rank,
+                                   const int32_t* __restrict__ b_of_row, int64_t nverts) {
   const BatchSetupArg& a = *ap;
   const int t = threadIdx.x;
   if (t < kBatchMax) {
     const bool ok = t < a.K && a.v[t] >= 0 && a.v[t] < nverts;
-    ctl->root_row[t] = ok ? rank[a.v[t]] : -1;
+    int row = ok ? rank[a.v[t]] : -1;
+    if (row >= 0 && b_of_row) row = b_of_row[row];
+    ctl->root_row[t] = row;
     ctl->root_lv[t] = t < a.K ? a.lv[t] : 0;
     ctl->prev_cnt[t] = 0;
   }
@@ -675,6 +669,115 @@ __global__ void batch_parent_kernel(const int32_t* __restrict__ lv, int64_t R,
 __global__ void set_entry_kernel(int64_t* p, int64_t i, int64_t value) { p[i] = value; }
 
 }  // namespace
+
+namespace {
+
+// Batch view of a group-reordered graph: rows renumbered in the global
+// degree order (the order the neighbour lists already follow).
+__global__ void bview_keys_kernel(const int32_t* __restrict__ mdeg, const int32_t* __restrict__ inv,
+                                  int64_t R, uint64_t* __restrict__ keys,
+                                  int32_t* __restrict__ rows) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < R;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    keys[r] = ((uint64_t)(0xFFFFFFFFu - (uint32_t)mdeg[r]) << 32) | (uint32_t)inv[r];
+    rows[r] = (int32_t)r;
+  }
+}
+
+__global__ void bview_maps_kernel(const int32_t* __restrict__ order, int64_t R,
+                                  const int32_t* __restrict__ inv,
+                                  const int32_t* __restrict__ mdeg,
+                                  const int64_t* __restrict__ row_ptr,
+                                  int32_t* __restrict__ b_of_row, int32_t* __restrict__ binv,
+                                  int32_t* __restrict__ bmdeg, int64_t* __restrict__ blen) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < R;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t r = order[k];
+    b_of_row[r] = (int32_t)k;
+    binv[k] = inv[r];
+    bmdeg[k] = mdeg[r];
+    blen[k] = row_ptr[r + 1] - row_ptr[r];
+  }
+}
+
+// Warp per view row: copies its list with the neighbours renumbered.
+__global__ void bview_copy_kernel(const int32_t* __restrict__ order, int64_t R,
+                                  const int64_t* __restrict__ row_ptr,
+                                  const int32_t* __restrict__ col,
+                                  const int32_t* __restrict__ b_of_row,
+                                  const int64_t* __restrict__ brow_ptr,
+                                  int32_t* __restrict__ bcol) {
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = gw; k < R; k += nwarps) {
+    const int32_t r = order[k];
+    const int64_t b = row_ptr[r], e = row_ptr[r + 1], o = brow_ptr[k];
+    for (int64_t j = b + lane; j < e; j += 32) bcol[o + (j - b)] = b_of_row[col[j]];
+  }
+}
+
+}  // namespace
+
+void ensure_batch_view(DeviceArena& arena, Graph& g, cudaStream_t s, int sms) {
+  if (!g.group_reorder || g.bview_built) return;
+  const Csr& c = g.csr;
+  const int64_t R = c.nrows;
+  const int B = 256;
+  uint64_t* k1 = arena_alloc<uint64_t>(arena, R, "view keys");
+  uint64_t* k2 = arena_alloc<uint64_t>(arena, R, "view keys");
+  int32_t* r1 = arena_alloc<int32_t>(arena, R, "view rows");
+  int32_t* order = arena_alloc<int32_t>(arena, R, "view order");
+  bview_keys_kernel<<<grid_for(R, B, sms, 8), B, 0, s>>>(c.mdeg, c.inv, R, k1, r1);
+  size_t tmp = 0;
+  check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k1, k2, r1, order, (int)R, 0, 64, s),
+             "view sort size");
+  void* t = arena.alloc(tmp, "view sort temp");
+  check_cuda(cub::DeviceRadixSort::SortPairs(t, tmp, k1, k2, r1, order, (int)R, 0, 64, s),
+             "view sort");
+  arena.free(t);
+  arena.free(k1);
+  arena.free(k2);
+  arena.free(r1);
+  Csr v;
+  v.nrows = R;
+  v.nedges = c.nedges;
+  v.max_degree = c.max_degree;
+  g.b_of_row = arena_alloc<int32_t>(arena, R, "view row map");
+  v.inv = arena_alloc<int32_t>(arena, R, "view inv");
+  v.mdeg = arena_alloc<int32_t>(arena, R, "view mdeg");
+  int64_t* blen = arena_alloc<int64_t>(arena, R, "view row lengths");
+  bview_maps_kernel<<<grid_for(R, B, sms, 8), B, 0, s>>>(order, R, c.inv, c.mdeg, c.row_ptr,
+                                                        g.b_of_row, v.inv, v.mdeg, blen);
+  v.row_ptr = arena_alloc<int64_t>(arena, R + 1, "view row ptr");
+  check_cuda(cudaMemsetAsync(v.row_ptr, 0, 8, s), "memset");
+  tmp = 0;
+  check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tmp, blen, v.row_ptr + 1, (int)R, s),
+             "view scan size");
+  t = arena.alloc(tmp, "view scan temp");
+  check_cuda(cub::DeviceScan::InclusiveSum(t, tmp, blen, v.row_ptr + 1, (int)R, s), "view scan");
+  arena.free(t);
+  arena.free(blen);
+  v.col = arena_alloc<int32_t>(arena, c.nedges, "view adjacency");
+  bview_copy_kernel<<<grid_for(R * 32, B, sms, 8), B, 0, s>>>(order, R, c.row_ptr, c.col,
+                                                               g.b_of_row, v.row_ptr, v.col);
+  check_cuda(cudaStreamSynchronize(s), "batch view");
+  arena.free(order);
+  g.bview = v;
+  g.bview_built = true;
+}
+
+void free_batch_view(DeviceArena& arena, Graph& g) {
+  if (!g.bview_built) return;
+  arena.free(g.bview.row_ptr);
+  arena.free(g.bview.col);
+  arena.free(g.bview.inv);
+  arena.free(g.bview.mdeg);
+  arena.free(g.b_of_row);
+  g.bview = Csr();
+  g.b_of_row = nullptr;
+  g.bview_built = false;
+}
 
 cudaEvent_t BatchState::event(size_t i) {
   while (ev.size() <= i) {
@@ -777,7 +880,7 @@ namespace {
 // top-down push at ev[0..3].
 void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
                   cudaGraphConditionalHandle cond, int use_cond, const cudaEvent_t* ev) {
-  const Csr& c = g.csr;
+  const Csr& c = batch_csr(g);
   const int B = 256;
   const unsigned nblk = (unsigned)std::max<int64_t>(bs.nblk, 1);
   if (ev) check_cuda(cudaEventRecord(ev[0], s), "event");
@@ -800,13 +903,13 @@ void launch_prologue(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
   batch_zero_kernel<<<grid_for(bs.R, 256, sms, 8), 256, 0, s>>>(
       static_cast<const BatchSetupArg*>(bs.d_arg));
   batch_setup_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, static_cast<const BatchSetupArg*>(bs.d_arg),
-                                             g.csr.rank, g.nverts);
+                                             g.csr.rank, g.b_of_row, g.nverts);
 }
 
 std::vector<const void*> graph_key_of(const Graph& g, const BatchState& bs, int sms) {
-  const Csr& c = g.csr;
+  const Csr& c = batch_csr(g);
   return {bs.ctl, bs.d_arg, bs.blk_cnt, bs.blk_deg, (const void*)(intptr_t)bs.nblk,
-          (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, c.rank,
+          (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, g.csr.rank, g.b_of_row,
           (const void*)(intptr_t)g.nverts, bs.queue, bs.qdeg, (const void*)(intptr_t)sms};
 }
 
@@ -831,7 +934,7 @@ void build_graph(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
     if (err == cudaSuccess)
       err = cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault);
     if (err == cudaSuccess) {
-      batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, g.csr.mdeg, cond, 1);
+      batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, batch_csr(g).mdeg, cond, 1);
       err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
     }
     cudaGraphNode_t node = nullptr;
@@ -877,7 +980,7 @@ void batch_reserve(DeviceArena& arena, const Graph& g, BatchState& bs) {
 void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t s,
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
                bool use_graph, b200bfs_batch_stats* stats) {
-  const Csr& c = g.csr;
+  const Csr& c = batch_csr(g);
   if (!bs.allocated || bs.R != c.nrows) batch_allocate(arena, g, bs);
   BatchSetupArg& a = *static_cast<BatchSetupArg*>(bs.h_arg);
   memset(&a, 0, sizeof(a));
@@ -1012,7 +1115,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
 
 void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream_t s, int sms,
                   int index) {
-  const Csr& c = g.csr;
+  const Csr& c = batch_csr(g);
   const int B = 256;
   int32_t* lv = st.queue;  // scratch of R + 1 entries (the single-source queue)
   batch_row_levels_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.planes, bs.R, bs.levels,

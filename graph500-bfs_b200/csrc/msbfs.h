@@ -109,6 +109,15 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
                int sms, const int64_t* roots, int k, int edgefactor, double alpha, double beta,
                bool use_graph, b200bfs_batch_stats* stats);
 
+// The graph the batched search runs on: g.csr, or for a group-reordered
+// graph its view in global degree order (hub rows together, so the masks the
+// bottom-up sweep probes most stay in a few cache lines).
+inline const Csr& batch_csr(const Graph& g) { return g.bview_built ? g.bview : g.csr; }
+// Builds that view once (no-op unless the graph is group-reordered); not
+// thread-safe: call it before concurrent batches.
+void ensure_batch_view(DeviceArena& arena, Graph& g, cudaStream_t s, int sms);
+void free_batch_view(DeviceArena& arena, Graph& g);
+
 // Allocates bs for g (level planes, masks, queue, control block) ahead of
 // its first batch.
 void batch_reserve(DeviceArena& arena, const Graph& g, BatchState& bs);

@@ -262,6 +262,12 @@ int b200bfs_server_add_graph(b200bfs_server* p, int scale, int edgefactor, uint6
     if (rc != B200BFS_OK) fail(rc);
     // Slots: as many as the budget admits, at least one.
     cudaSetDevice(h->e.device);
+    try {
+      b200bfs::ensure_batch_view(h->e.arena, h->e.g, h->e.stream, h->e.sms);
+    } catch (const b200bfs::Error& x) {
+      h->e.last_error = x.msg;
+      fail(x.code);
+    }
     for (int i = 0; i < s.cfg.slots_per_graph; ++i) {
       std::unique_ptr<b200bfs::Slot> sl(new b200bfs::Slot());
       try {

@@ -241,9 +241,36 @@ int b200bfs_get_level_stats(b200bfs_handle* h, b200bfs_level_stats* out, int max
 /* Statistics of the last run. */
 int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
 
+/* ------------------------------ engine tuner ------------------------------ */
+
+enum {
+  B200BFS_TUNE_FORMS = 1 << 0,        /* bottom-up and top-down kernel forms   */
+  B200BFS_TUNE_BATCH_ALPHA = 1 << 1   /* alpha of b200bfs_run_batch            */
+};
+
+typedef struct b200bfs_tune_report {
+  int32_t bu_kernel;             /* chosen "bu_kernel" option                 */
+  int32_t td_kernel;             /* chosen "td_kernel" option                 */
+  double batch_alpha;            /* chosen "batch_alpha" option               */
+  double single_ms;              /* mean search time with the chosen forms    */
+  double batch_ms;               /* batch time with the chosen alpha          */
+  int32_t searches;              /* single-source searches the tuner ran      */
+  int32_t batches;               /* batches the tuner ran                     */
+} b200bfs_tune_report;
+
+/* No counterpart in the reference, whose equivalents are compile-time
+ * constants of parameters.h: picks, for the resident graph, the bottom-up
+ * and top-down kernel forms (timing each on up to 16 of the roots with
+ * alpha/beta) and the batched search's alpha (timing 64-root batches with
+ * 10..400), and keeps the fastest in the engine's options ("bu_kernel",
+ * "td_kernel", "batch_alpha").  what: B200BFS_TUNE_* bits.  Levels and
+ * parent validity do not depend on the choices.  out may be NULL. */
+int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, int edgefactor,
+                        double alpha, double beta, int what, b200bfs_tune_report* out);
+
 /* Engine tuning knobs (no counterpart in the reference, whose equivalents
  * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
- * kernel form), "td_kernel" (1..4, top-down kernel form; 4 picks per level), "bu_probe" (1..64,
+ * kernel form), "td_kernel" (1..5, top-down kernel form; 4 picks per level), "bu_probe" (1..64,
  * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
  * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2),
  * "batch_graph" (1: b200bfs_run_batch runs its level loop as a CUDA graph on

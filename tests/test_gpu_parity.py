@@ -244,7 +244,7 @@ def test_hbm_budget_admission(built):
     e.close()
 
 
-@pytest.mark.parametrize("bu,td", [(1, 1), (2, 2), (3, 1), (4, 2), (4, 3), (4, 4)])
+@pytest.mark.parametrize("bu,td", [(1, 1), (2, 2), (3, 1), (4, 2), (4, 3), (4, 4), (4, 5)])
 def test_kernel_forms_agree(engine, oracle_graphs, bu, td):
     """Every bottom-up / top-down kernel form gives the reference levels."""
     edges, g = oracle_graphs(18)
@@ -258,4 +258,28 @@ def test_kernel_forms_agree(engine, oracle_graphs, bu, td):
     finally:
         engine.set_option("bu_kernel", 4)
         engine.set_option("td_kernel", 4)
+        engine.end()
+
+
+def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
+    """b200bfs_tune_engine picks kernel forms and the batch alpha by timing;
+    searches and batches with its choices still give the oracle's levels."""
+    edges, g = oracle_graphs(18)
+    engine.generate_graph(18, 16)
+    engine.prepare(16)
+    roots = O.find_roots(g.has_edge(), 1 << 18, 8)
+    try:
+        rep = engine.tune_engine(roots)
+        assert 1 <= rep.bu_kernel <= 4 and rep.td_kernel in (1, 3, 4, 5)
+        assert rep.batch_alpha in (10.0, 20.0, 30.0, 50.0, 100.0, 200.0, 400.0)
+        assert rep.searches > 0 and rep.batches == 14 and rep.single_ms > 0 and rep.batch_ms > 0
+        _check_search(engine, edges, g, roots[:3])
+        engine.run_batch(roots, 16, 0.0)  # alpha <= 0: the tuned batch alpha
+        for i, r in enumerate(roots):
+            engine.batch_select(i)
+            assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(int(r)))
+    finally:
+        engine.set_option("bu_kernel", 4)
+        engine.set_option("td_kernel", 4)
+        engine.set_option("batch_alpha", 30)
         engine.end()
