@@ -90,7 +90,7 @@ __global__ void root_kernel(int64_t root, const int32_t* __restrict__ rank,
 // kWarpSearch: the tile's first row is found by a 32-way warp search
 // (log32 rounds of coalesced loads) instead of lane 0's binary search.
 template <bool kWarpSearch>
-__global__ void __launch_bounds__(256) td_expand_kernel(
+__device__ __forceinline__ void td_expand_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
@@ -230,8 +230,8 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
 // probes, back to back: kWords * 2 independent loads are in flight per lane
 // instead of one dependent chain.  Rows unresolved after 8 probes are swept
 // by the whole warp as in bu_kernel.
-template <int kWords, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
+template <int kWords>
+__device__ __forceinline__ void bu_wide_body(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
     const int32_t* __restrict__ inv, int64_t* __restrict__ pred, int64_t level,
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(256) td_wide_kernel(
 // has an edge) mark their start positions in a 32-slot array and a
 // prefix-max over the lanes gives each entry its row, so frontiers of many
 // short rows (the tail levels) do not walk the degree prefix row by row.
-__global__ void __launch_bounds__(256) td_chunk_kernel(
+__device__ __forceinline__ void td_chunk_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(256) td_chunk_kernel(
 
 // Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
 // vertices, their CSR degrees and their pre-dedup degrees.
-__global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
+__device__ __forceinline__ void frontier_count_body(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
     int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
@@ -565,11 +565,10 @@ __global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
 }
 
 // Frontier pass 2: exclusive scan of the block partials (single block).
-__global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict__ blk_cnt,
-                                                             int64_t* __restrict__ blk_deg,
-                                                             int64_t nblk,
-                                                             int64_t* __restrict__ qdeg,
-                                                             Counters* __restrict__ ctr) {
+__device__ __forceinline__ void frontier_scan_body(int64_t* __restrict__ blk_cnt,
+                                                   int64_t* __restrict__ blk_deg, int64_t nblk,
+                                                   int64_t* __restrict__ qdeg,
+                                                   Counters* __restrict__ ctr) {
   __shared__ int64_t s_a[32], s_b[32];
   const int t = threadIdx.x;
   const int64_t per = (nblk + blockDim.x - 1) / blockDim.x;
@@ -612,7 +611,7 @@ __global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict
 }
 
 // Frontier pass 3: write the queue in vertex order with its degree prefix.
-__global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
+__device__ __forceinline__ void frontier_write_body(
     const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
     int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
@@ -661,6 +660,56 @@ __global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
   }
 }
 
+// Kernels of the host-driven level loop: thin wrappers around the bodies
+// above, which the device-driven loop (below) shares.
+template <bool kWarpSearch>
+__global__ void __launch_bounds__(256) td_expand_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  td_expand_body<kWarpSearch>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
+}
+
+template <int kWords, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
+    const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
+    const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ inv, int64_t* __restrict__ pred, int64_t level,
+    Counters* __restrict__ ctr) {
+  bu_wide_body<kWords>(cur, nxt, W, row_ptr, col, inv, pred, level, ctr);
+}
+
+__global__ void __launch_bounds__(256) td_chunk_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
+}
+
+__global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
+    const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
+    int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
+    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
+  frontier_count_body(nw, old, fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+}
+
+__global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict__ blk_cnt,
+                                                             int64_t* __restrict__ blk_deg,
+                                                             int64_t nblk,
+                                                             int64_t* __restrict__ qdeg,
+                                                             Counters* __restrict__ ctr) {
+  frontier_scan_body(blk_cnt, blk_deg, nblk, qdeg, ctr);
+}
+
+__global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
+    const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
+    const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
+    int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
+  frontier_write_body(fr, W, row_ptr, blk_cnt, blk_deg, queue, qdeg);
+}
+
 __global__ void clear_counters_kernel(Counters* ctr) {
   ctr->nq = 0;
   ctr->nq_edges = 0;
@@ -674,6 +723,211 @@ __global__ void levels_kernel(const int64_t* __restrict__ pred, int64_t n,
     const int64_t p = pred[i];
     lv[i] = (p == -1) ? -1 : (int32_t)(((uint64_t)p >> 48) & 0xFFFF);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Device-driven level loop (engine option single_graph): the same kernels,
+// with the state that run_bfs_core keeps in host variables (level, direction,
+// growing, current bitmap, counts, auto_tuning_data) in a device control
+// block.  Every level launches the same sequence; the kernels whose step does
+// not apply to the level return at once, and sg_control_kernel applies the
+// switch rule of bfs.hpp:3413-3457 exactly as the host loop does (same
+// integer and double arithmetic) and sets the WHILE condition of the graph.
+
+__global__ void sg_root_kernel(const SgArg* __restrict__ a, const int32_t* __restrict__ rank,
+                               const int64_t* __restrict__ row_ptr, int64_t* __restrict__ pred,
+                               uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1,
+                               int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
+                               Counters* ctr, SingleCtl* __restrict__ c) {
+  const int64_t root = a->root;
+  pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
+  const int32_t r = rank[root];
+  memset(ctr, 0, sizeof(Counters));
+  if (r >= 0) {
+    vis0[r >> 5] |= 1u << (r & 31);
+    vis1[r >> 5] |= 1u << (r & 31);
+    queue[0] = r;
+    qdeg[0] = 0;
+    qdeg[1] = row_ptr[r + 1] - row_ptr[r];
+    ctr->qsize = 1;
+    ctr->qedges = qdeg[1];
+  } else {
+    ctr->qsize = 0;
+    qdeg[0] = 0;
+  }
+  memset(c, 0, sizeof(SingleCtl));
+  c->level = a->root_level;
+  c->next_forward = 1;
+  c->growing = 1;
+  c->visited = 1;
+  c->qsize = 1;
+  for (int i = 0; i < 9; ++i) c->at[i] = a->at[i];
+}
+
+// Level start (host loop: ++level, at[8], prev_nq, forward, clear counters).
+__global__ void sg_begin_kernel(SingleCtl* __restrict__ c, const SgArg* __restrict__ a,
+                                Counters* __restrict__ ctr) {
+  if (c->done) return;
+  ++c->level;
+  if (c->level > kMaxLevel) {
+    c->done = 3;
+    return;
+  }
+  if (a->want_at) c->at[8] = c->level;  // AUTO_LEVEL
+  c->prev_nq = c->global_nq_size;
+  c->forward = c->next_forward;
+  ctr->nq = 0;
+  ctr->nq_edges = 0;
+  ctr->scanned = 0;
+}
+
+// kForm 1/5: td_expand (lane or warp search); 3: td_chunk.  td_form is the
+// engine option (4 = 5 while growing, 3 after).
+template <int kForm>
+__global__ void __launch_bounds__(256) sg_td_kernel(
+    const SingleCtl* __restrict__ c, int td_form, const int32_t* __restrict__ queue,
+    const int64_t* __restrict__ qdeg, const Counters* __restrict__ ctr,
+    const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ inv, uint32_t* const* __restrict__ vis_pp,
+    int64_t* __restrict__ pred) {
+  if (c->done || !c->forward) return;
+  const int form = td_form == 4 ? (c->growing ? 5 : 3) : td_form;
+  if (form != kForm) return;
+  uint32_t* vis = vis_pp[c->cur];
+  if (kForm == 3)
+    td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
+  else
+    td_expand_body<kForm == 5>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
+}
+
+__global__ void __launch_bounds__(256, 4) sg_bu_kernel(
+    const SingleCtl* __restrict__ c, int64_t W, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    uint32_t* const* __restrict__ vis_pp, int64_t* __restrict__ pred,
+    Counters* __restrict__ ctr) {
+  if (c->done || c->forward) return;
+  const int cur = c->cur;
+  bu_wide_body<4>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, inv, pred, c->level, ctr);
+}
+
+// kAfterBu = false: after a top-down level; true: after a bottom-up level
+// whose next level is top-down (the bitmaps have swapped by then).
+template <bool kAfterBu>
+__global__ void __launch_bounds__(kWordsPerBlock) sg_count_kernel(
+    const SingleCtl* __restrict__ c, uint32_t* const* __restrict__ vis_pp,
+    uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ mdeg, int64_t* __restrict__ blk_cnt,
+    int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
+  if (c->done) return;
+  if (kAfterBu ? (c->forward || !c->next_forward) : !c->forward) return;
+  const int cur = c->cur;
+  frontier_count_body(vis_pp[cur], vis_pp[cur ^ 1], fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+}
+
+__global__ void __launch_bounds__(1024) sg_scan_kernel(const SingleCtl* __restrict__ c,
+                                                       int64_t* __restrict__ blk_cnt,
+                                                       int64_t* __restrict__ blk_deg,
+                                                       int64_t nblk, int64_t* __restrict__ qdeg,
+                                                       Counters* __restrict__ ctr) {
+  if (c->done || !c->next_forward) return;
+  frontier_scan_body(blk_cnt, blk_deg, nblk, qdeg, ctr);
+}
+
+__global__ void __launch_bounds__(kWordsPerBlock) sg_write_kernel(
+    const SingleCtl* __restrict__ c, const uint32_t* __restrict__ fr, int64_t W,
+    const int64_t* __restrict__ row_ptr, const int64_t* __restrict__ blk_cnt,
+    const int64_t* __restrict__ blk_deg, int32_t* __restrict__ queue,
+    int64_t* __restrict__ qdeg) {
+  if (c->done || !c->next_forward) return;
+  frontier_write_body(fr, W, row_ptr, blk_cnt, blk_deg, queue, qdeg);
+}
+
+// Level end: the host loop's bookkeeping and switch rule (bfs.hpp:3413-3457).
+__global__ void sg_control_kernel(SingleCtl* __restrict__ c, const SgArg* __restrict__ a,
+                                  const Counters* __restrict__ ctr, int64_t R, int64_t W,
+                                  int64_t nedges, int64_t nrows, int force_direction,
+                                  cudaGraphConditionalHandle cond) {
+  if (c->done) {
+    cudaGraphSetConditional(cond, 0u);
+    return;
+  }
+  const bool forward = c->forward != 0;
+  const int64_t nq = (int64_t)ctr->nq;
+  c->global_nq_size = nq;
+  SgRec rec;
+  rec.level = (int32_t)c->level;
+  if (forward) {
+    c->global_nq_edges = (int64_t)ctr->nq_edges;
+    const int64_t e_td = (int64_t)ctr->qedges;
+    const int64_t b = 16 * c->qsize + 8 * e_td + 12 * nq;
+    c->scanned_td += e_td;
+    c->td_bytes += b;
+    c->bytes += b;
+    ++c->num_td;
+    rec.bottom_up = 0;
+    rec.input = c->qsize;
+    rec.scanned = e_td;
+    rec.bytes = b;
+  } else {
+    const int64_t unvisited = R - c->visited;
+    const int64_t sc = (int64_t)ctr->scanned;
+    const int64_t b = 3 * (W * 4) + 16 * unvisited + 8 * sc + 12 * nq;
+    c->scanned_bu += sc;
+    c->bu_bytes += b;
+    c->bytes += b;
+    ++c->num_bu;
+    if (c->level < 64) c->bu_mask |= 1ull << c->level;
+    c->cur ^= 1;
+    rec.bottom_up = 1;
+    rec.input = unvisited;
+    rec.scanned = sc;
+    rec.bytes = b;
+  }
+  rec.discovered = nq;
+  if (c->nrec < kSgHist) c->rec[c->nrec] = rec;
+  ++c->nrec;
+  c->visited += nq;
+  if (nq == 0) {
+    c->done = 1;
+    cudaGraphSetConditional(cond, 0u);
+    return;
+  }
+  const double alpha = a->alpha, beta = a->beta;
+  const bool at = a->want_at != 0;
+  bool next_forward = c->next_forward != 0;
+  if (c->growing && nq > c->prev_nq) {
+    if (forward) {
+      if (c->global_nq_edges > (int64_t)(nedges / alpha)) {
+        next_forward = false;
+        if (at) {
+          c->at[0] = c->global_nq_edges;  // AUTO_GLOBAL_NQ_EDGES
+          c->at[1] = nedges;              // AUTO_NUM_GLOBAL_EDGES
+          c->at[2] = c->level;            // AUTO_T2B_LEVEL
+        }
+      } else if (at) {
+        c->at[6] = c->global_nq_edges;  // AUTO_PRE_GLOBAL_NQ_EDGES
+      }
+    }
+  } else {
+    if (!forward) {
+      if (nq < (int64_t)(nrows / (beta * a->edgefactor * 2.0))) {
+        next_forward = true;
+        c->growing = 0;
+        if (at) {
+          c->at[3] = nq;        // AUTO_GLOBAL_NQ_SIZE
+          c->at[4] = nrows;     // AUTO_NUM_GLOBAL_VERTS
+          c->at[5] = c->level;  // AUTO_B2T_LEVEL
+        }
+      } else if (at) {
+        c->at[7] = nq;  // AUTO_PRE_GLOBAL_NQ_SIZE
+      }
+    }
+  }
+  if (force_direction == 1) next_forward = true;
+  if (force_direction == 2) next_forward = false;
+  c->next_forward = next_forward ? 1 : 0;
+  if (next_forward) c->qsize = nq;
+  cudaGraphSetConditional(cond, 1u);
 }
 
 }  // namespace
@@ -694,6 +948,12 @@ void BfsState::allocate(DeviceArena& arena, const Graph& g) {
   pred = arena_alloc<int64_t>(arena, pred_size + 2, "pred");
   ctr = arena_alloc<Counters>(arena, 1, "counters");
   check_cuda(cudaMallocHost(&hctr, sizeof(Counters)), "pinned counters");
+  sctl = arena_alloc<SingleCtl>(arena, 1, "search control block");
+  sarg = arena_alloc<SgArg>(arena, 1, "search arguments");
+  d_vis = arena_alloc<uint32_t*>(arena, 2, "bitmap pointers");
+  check_cuda(cudaMemcpy(d_vis, vis, sizeof(vis), cudaMemcpyHostToDevice), "bitmap pointers");
+  check_cuda(cudaMallocHost(&hsctl, sizeof(SingleCtl)), "pinned control block");
+  check_cuda(cudaMallocHost(&hsarg, sizeof(SgArg)), "pinned arguments");
   allocated = true;
 }
 
@@ -709,7 +969,22 @@ cudaEvent_t BfsState::event(size_t i) {
 void BfsState::release(DeviceArena& arena) {
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
   ev.clear();
+  if (sgexec) cudaGraphExecDestroy(sgexec);
+  if (sgraph) cudaGraphDestroy(sgraph);
+  sgexec = nullptr;
+  sgraph = nullptr;
+  skey.clear();
   if (!allocated) return;
+  arena.free(sctl);
+  arena.free(sarg);
+  arena.free(d_vis);
+  d_vis = nullptr;
+  cudaFreeHost(hsctl);
+  cudaFreeHost(hsarg);
+  sctl = nullptr;
+  sarg = nullptr;
+  hsctl = nullptr;
+  hsarg = nullptr;
   arena.free(vis[0]);
   arena.free(vis[1]);
   arena.free(fr);
@@ -724,10 +999,169 @@ void BfsState::release(DeviceArena& arena) {
   allocated = false;
 }
 
+namespace {
+
+int chunk_blocks_per_sm() {
+  static int per_sm = 0;
+  if (!per_sm &&
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_chunk_kernel, 256, 0) !=
+          cudaSuccess)
+    per_sm = 4;
+  return std::max(per_sm, 1);
+}
+
+// One level of the device-driven loop (captured into the WHILE body).
+void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
+                     int force_direction, cudaGraphConditionalHandle cond) {
+  const Csr& c = g.csr;
+  const int B = 256;
+  const unsigned nblk = (unsigned)st.nblk;
+  sg_begin_kernel<<<1, 1, 0, s>>>(st.sctl, st.sarg, st.ctr);
+  sg_td_kernel<1><<<sms * 8, B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg, st.ctr, c.row_ptr,
+                                         c.col, c.inv, st.d_vis, st.pred);
+  sg_td_kernel<5><<<sms * 8, B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg, st.ctr, c.row_ptr,
+                                         c.col, c.inv, st.d_vis, st.pred);
+  sg_td_kernel<3><<<sms * chunk_blocks_per_sm(), B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg,
+                                                             st.ctr, c.row_ptr, c.col, c.inv,
+                                                             st.d_vis, st.pred);
+  sg_bu_kernel<<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.inv, st.d_vis, st.pred,
+                                     st.ctr);
+  sg_count_kernel<false><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
+                                                         c.row_ptr, c.mdeg, st.blk_cnt,
+                                                         st.blk_deg, st.ctr);
+  sg_control_kernel<<<1, 1, 0, s>>>(st.sctl, st.sarg, st.ctr, st.R, st.W, c.nedges, c.nrows,
+                                    force_direction, cond);
+  sg_count_kernel<true><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
+                                                        c.row_ptr, c.mdeg, st.blk_cnt,
+                                                        st.blk_deg, st.ctr);
+  sg_scan_kernel<<<1, 1024, 0, s>>>(st.sctl, st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
+  sg_write_kernel<<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_cnt,
+                                                  st.blk_deg, st.queue, st.qdeg);
+}
+constexpr int kSgLevelLaunches = 11;
+
+std::vector<const void*> sg_key(const Graph& g, const BfsState& st, int sms, int td_form,
+                                int force_direction) {
+  const Csr& c = g.csr;
+  return {st.sctl, st.sarg, st.d_vis, st.ctr, st.fr, st.queue, st.qdeg, st.blk_cnt, st.blk_deg,
+          st.pred, st.vis[0], st.vis[1], c.row_ptr, c.col, c.inv, c.rank, c.mdeg,
+          (const void*)(intptr_t)st.W, (const void*)(intptr_t)st.R,
+          (const void*)(intptr_t)st.pred_size, (const void*)(intptr_t)c.nedges,
+          (const void*)(intptr_t)sms, (const void*)(intptr_t)td_form,
+          (const void*)(intptr_t)force_direction};
+}
+
+// [init, root] then WHILE(level); the control kernel sets the condition.
+void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
+                    int force_direction) {
+  if (st.sgexec) cudaGraphExecDestroy(st.sgexec);
+  if (st.sgraph) cudaGraphDestroy(st.sgraph);
+  st.sgexec = nullptr;
+  st.sgraph = nullptr;
+  const Csr& c = g.csr;
+  check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+  init_kernel<<<grid_for(std::max(st.pred_size / 2, st.W), 256, sms, 8), 256, 0, s>>>(
+      st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R);
+  sg_root_kernel<<<1, 1, 0, s>>>(st.sarg, c.rank, c.row_ptr, st.pred, st.vis[0], st.vis[1],
+                                 st.queue, st.qdeg, st.ctr, st.sctl);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaGraph_t cg = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  cudaError_t err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+  if (err == cudaSuccess)
+    err = cudaGraphConditionalHandleCreate(&cond, cg, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t node = nullptr;
+  cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+  p.conditional.handle = cond;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  if (err == cudaSuccess) err = cudaGraphAddNode(&node, cg, deps, nd, &p);
+  if (err == cudaSuccess)
+    err = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+  cudaGraph_t body = err == cudaSuccess ? p.conditional.phGraph_out[0] : nullptr;
+  cudaGraph_t outer = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &outer);
+  if (err == cudaSuccess) err = e2;
+  st.sgraph = outer;
+  if (err == cudaSuccess) {
+    err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      sg_launch_level(g, st, s, sms, td_form, force_direction, cond);
+      cudaGraph_t b2 = nullptr;
+      err = cudaStreamEndCapture(s, &b2);
+    }
+  }
+  if (err == cudaSuccess) err = cudaGraphInstantiate(&st.sgexec, st.sgraph, 0);
+  if (err != cudaSuccess) {
+    if (st.sgraph) cudaGraphDestroy(st.sgraph);
+    st.sgraph = nullptr;
+    st.sgexec = nullptr;
+    cudaGetLastError();
+    check_cuda(err, "search level-loop graph");
+  }
+  st.skey = sg_key(g, st, sms, td_form, force_direction);
+}
+
+// run_bfs_core with the level loop on the device.
+void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
+                        int64_t root_level, int edgefactor, double alpha, double beta,
+                        int64_t* at, const RunOptions& opt, b200bfs_run_stats* stats) {
+  if (!st.sgexec || st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction))
+    sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction);
+  SgArg& a = *st.hsarg;
+  a.root = root;
+  a.root_level = root_level;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.edgefactor = edgefactor;
+  a.want_at = at != nullptr;
+  for (int i = 0; i < 9; ++i) a.at[i] = at ? at[i] : -1;
+  check_cuda(cudaMemcpyAsync(st.sarg, st.hsarg, sizeof(SgArg), cudaMemcpyHostToDevice, s),
+             "search arguments");
+  check_cuda(cudaGraphLaunch(st.sgexec, s), "search graph");
+  check_cuda(cudaMemcpyAsync(st.hsctl, st.sctl, sizeof(SingleCtl), cudaMemcpyDeviceToHost, s),
+             "control block");
+  check_cuda(cudaStreamSynchronize(s), "search");
+  const SingleCtl& c = *st.hsctl;
+  if (c.done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
+  if (at)
+    for (int i = 0; i < 9; ++i) at[i] = c.at[i];
+  st.levels.clear();
+  for (int i = 0; i < std::min(c.nrec, kSgHist); ++i) {
+    const SgRec& r = c.rec[i];
+    st.levels.push_back({r.level, r.bottom_up, r.input, r.discovered, r.scanned, r.bytes, 0.0});
+  }
+  if (stats) {
+    b200bfs_run_stats rs;
+    memset(&rs, 0, sizeof(rs));
+    rs.levels = (int32_t)c.level;
+    rs.num_td_levels = (int32_t)c.num_td;
+    rs.num_bu_levels = (int32_t)c.num_bu;
+    rs.bu_level_mask = c.bu_mask;
+    rs.visited = c.visited;
+    rs.edges_scanned_td = c.scanned_td;
+    rs.edges_scanned_bu = c.scanned_bu;
+    rs.td_bytes = c.td_bytes;
+    rs.bu_bytes = c.bu_bytes;
+    rs.algorithmic_bytes = c.bytes + 8 * st.pred_size;
+    rs.kernel_launches = 2 + kSgLevelLaunches * (int)(c.num_td + c.num_bu);
+    *stats = rs;
+  }
+}
+
+}  // namespace
+
 // The level loop with the reference's direction switch.
 void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                   int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
                   const RunOptions& opt, b200bfs_run_stats* stats) {
+  if (opt.single_graph && opt.bu_kernel == 4 && opt.td_kernel != 2) {
+    run_bfs_core_graph(g, st, s, sms, root, root_level, edgefactor, alpha, beta, at, opt, stats);
+    return;
+  }
   const Csr& c = g.csr;
   const int B = 256;
   b200bfs_run_stats rs;
@@ -755,12 +1189,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   const int bu_wide_grid = sms * 8;
   // the chunked top-down form splits the work evenly over its warps, so its
   // grid is exactly the resident blocks (one wave)
-  static int chunk_per_sm = 0;
-  if (!chunk_per_sm &&
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&chunk_per_sm, td_chunk_kernel, B, 0) !=
-          cudaSuccess)
-    chunk_per_sm = 4;
-  const int td_chunk_grid = sms * std::max(chunk_per_sm, 1);
+  const int td_chunk_grid = sms * chunk_blocks_per_sm();
   for (;;) {
     ++level;
     if (level > kMaxLevel) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};

@@ -16,6 +16,32 @@ struct Counters {
   int pad;
 };
 
+// Device-driven level loop of the single-source search (CUDA graph mode).
+constexpr int kSgHist = 128;  // per-level records kept on the device
+struct SgRec {
+  int32_t level, bottom_up;
+  int64_t input, discovered, scanned, bytes;
+};
+// Per-search arguments, written by the host before each graph launch.
+struct SgArg {
+  long long root, root_level;
+  double alpha, beta;
+  int edgefactor, want_at;
+  long long at[9];
+};
+// Control block: the state the host loop keeps in local variables.
+struct SingleCtl {
+  long long level;
+  int forward, next_forward, growing, cur, done, pad;
+  long long global_nq_size, global_nq_edges, visited, qsize, prev_nq;
+  long long at[9];
+  long long num_td, num_bu;
+  unsigned long long bu_mask;
+  long long scanned_td, scanned_bu, td_bytes, bu_bytes, bytes;
+  int nrec, pad2;
+  SgRec rec[kSgHist];
+};
+
 struct BfsState {
   bool allocated = false;
   int64_t R = 0, W = 0, pred_size = 0, nblk = 0;
@@ -30,6 +56,15 @@ struct BfsState {
   Counters* hctr = nullptr;               // pinned mirror
   std::vector<cudaEvent_t> ev;            // per-level kernel timing events
   std::vector<b200bfs_level_stats> levels;  // per-level record of the last search
+  // device-driven level loop (graph mode)
+  SingleCtl* sctl = nullptr;
+  SingleCtl* hsctl = nullptr;             // pinned mirror
+  SgArg* sarg = nullptr;
+  uint32_t** d_vis = nullptr;             // device copy of vis[2]
+  SgArg* hsarg = nullptr;                 // pinned staging
+  cudaGraph_t sgraph = nullptr;
+  cudaGraphExec_t sgexec = nullptr;
+  std::vector<const void*> skey;
 
   cudaEvent_t event(size_t i);            // creates events on demand
 
@@ -50,6 +85,10 @@ struct RunOptions {
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
   int batch_graph = 1;      // batched search: level loop in a CUDA graph (0: host loop)
+  // single-source search: level loop on the device in a CUDA graph (default
+  // forms only: bottom-up form 4, top-down forms 1, 3, 4, 5); 0: host loop
+  // with per-level kernel timings
+  int single_graph = 0;
   double batch_alpha = 30;  // batched search: alpha used when the caller passes alpha <= 0
 };
 

@@ -529,6 +529,9 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "bu_probe") {
       require(value >= 1 && value <= 64, B200BFS_ERR_INVALID, "bu_probe must be 1..64");
       e.opt.bu_probe = (int)value;
+    } else if (n == "single_graph") {
+      require(value == 0 || value == 1, B200BFS_ERR_INVALID, "single_graph must be 0 or 1");
+      e.opt.single_graph = (int)value;
     } else if (n == "batch_graph") {
       require(value == 0 || value == 1, B200BFS_ERR_INVALID, "batch_graph must be 0 or 1");
       e.opt.batch_graph = (int)value;

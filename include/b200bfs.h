@@ -273,6 +273,10 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * kernel form), "td_kernel" (1..5, top-down kernel form; 4 picks per level), "bu_probe" (1..64,
  * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
  * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2),
+ * "single_graph" (1: b200bfs_run runs its level loop as a CUDA graph on the
+ * device, one host synchronisation per search, with bottom-up form 4 and
+ * top-down forms 1, 3, 4 or 5; per-level kernel times are then not
+ * recorded; 0: host loop, the default),
  * "batch_graph" (1: b200bfs_run_batch runs its level loop as a CUDA graph on
  * the device, 0: the host launches each level and per-level times are
  * recorded), "batch_alpha" (the alpha b200bfs_run_batch uses when given

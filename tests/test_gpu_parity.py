@@ -283,3 +283,46 @@ def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
         engine.set_option("td_kernel", 4)
         engine.set_option("batch_alpha", 30)
         engine.end()
+
+
+@pytest.mark.parametrize("alpha,beta,flags", [(10.0, 14.0, 0), (1e-9, 14.0, 0), (1e9, 14.0, 0),
+                                              (2.0, 100.0, 0), (30.0, 2.0, 0), (10.0, 14.0, 3)])
+def test_device_level_loop_matches_host_loop(engine, oracle_graphs, alpha, beta, flags):
+    """The level loop run on the device (one CUDA graph per search) applies
+    the same switch rule: levels, auto_tuning_data, run statistics and
+    per-level records equal the host loop's and the oracle's."""
+    import b200bfs
+
+    edges, g = oracle_graphs(16)
+    engine.generate_graph(16, 16, flags=flags)
+    engine.prepare(16, alpha, beta)
+    if flags & b200bfs.BUILD_COREBFS:
+        roots = O.find_roots(O.Core(g).has_edge(), 1 << 16, 4)
+    else:
+        roots = O.find_roots(g.has_edge(), 1 << 16, 4)
+    keys = ("levels", "num_td_levels", "num_bu_levels", "bu_level_mask", "visited",
+            "edges_scanned_td", "edges_scanned_bu", "algorithmic_bytes", "td_bytes", "bu_bytes")
+    try:
+        for r in roots:
+            r = int(r)
+            engine.set_option("single_graph", 0)
+            at_h = engine.run(r, 16, alpha, beta)
+            st_h = engine.run_stats()
+            lv_h = [{k: v for k, v in x.items() if k != "ms"} for x in engine.level_stats()]
+            engine.set_option("single_graph", 1)
+            at_d = engine.run(r, 16, alpha, beta)
+            st_d = engine.run_stats()
+            lv_d = [{k: v for k, v in x.items() if k != "ms"} for x in engine.level_stats()]
+            assert np.array_equal(at_h, at_d)
+            for k in keys:
+                assert getattr(st_h, k) == getattr(st_d, k), k
+            assert lv_h == lv_d
+            assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r))
+            err, cnt = engine.validate(r)
+            assert err == 0
+        if not flags:
+            engine.set_option("single_graph", 1)
+            _check_search(engine, edges, g, roots, alpha, beta)
+    finally:
+        engine.set_option("single_graph", 0)
+        engine.end()
