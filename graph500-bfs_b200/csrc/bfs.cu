@@ -43,16 +43,20 @@ __device__ __forceinline__ void warp_inclusive_scan2(int64_t& a, int64_t& b) {
   }
 }
 
+// initialize_memory (bfs.hpp:315-349).  pred is filled with -1 only when it
+// is not already clean (see BfsState::pred_clean); the bitmaps always.
 __global__ void init_kernel(int64_t* __restrict__ pred, int64_t pred_size,
                             uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1, int64_t W,
-                            int64_t R) {
+                            int64_t R, int fill_pred) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  // pred in 16-byte stores
-  longlong2* p2 = reinterpret_cast<longlong2*>(pred);
-  const int64_t n2 = pred_size >> 1;
-  for (int64_t i = t0; i < n2; i += stride) p2[i] = make_longlong2(-1, -1);
-  if (t0 == 0 && (pred_size & 1)) pred[pred_size - 1] = -1;
+  if (fill_pred) {
+    // pred in 16-byte stores
+    longlong2* p2 = reinterpret_cast<longlong2*>(pred);
+    const int64_t n2 = pred_size >> 1;
+    for (int64_t i = t0; i < n2; i += stride) p2[i] = make_longlong2(-1, -1);
+    if (t0 == 0 && (pred_size & 1)) pred[pred_size - 1] = -1;
+  }
   for (int64_t w = t0; w < W; w += stride) {
     // bits at or beyond R are padding and start "visited"
     int64_t first = w * 32;
@@ -63,11 +67,14 @@ __global__ void init_kernel(int64_t* __restrict__ pred, int64_t pred_size,
   }
 }
 
-__global__ void root_kernel(int64_t root, const int32_t* __restrict__ rank,
+// prev_root: the previous search's root entry, cleared first (it is not
+// covered by the reset of unvisited rows when it is not a row of the CSR).
+__global__ void root_kernel(int64_t root, int64_t prev_root, const int32_t* __restrict__ rank,
                             const int64_t* __restrict__ row_ptr, int64_t* __restrict__ pred,
                             uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1,
                             int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
                             Counters* ctr) {
+  if (prev_root >= 0) pred[prev_root] = -1;
   pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
   int32_t r = rank[root];
   memset(ctr, 0, sizeof(Counters));
@@ -85,11 +92,33 @@ __global__ void root_kernel(int64_t root, const int32_t* __restrict__ rank,
   }
 }
 
+// End of a search: rows the search did not reach get pred = -1, so pred
+// holds exactly this search's result without a full re-initialisation at
+// the start of the next one (vertices without edges keep the -1 of the
+// first fill; rows reached by an earlier search and not by this one are the
+// only stale entries, and they are exactly the rows reset here).
+__global__ void reset_unvisited_kernel(const uint32_t* __restrict__ vis, int64_t W,
+                                       const int32_t* __restrict__ inv,
+                                       int64_t* __restrict__ pred) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < W;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t un = ~vis[w];  // padding bits beyond R are set, so never reset
+    while (un) {
+      const int b = __ffs(un) - 1;
+      un &= un - 1;
+      pred[inv[w * 32 + b]] = -1;
+    }
+  }
+}
+
 // Edge-balanced top-down expansion.  Frontier queue[0..qsize) with
 // qdeg[i] = sum of degrees of queue[0..i) (qdeg[qsize] = total).
 // kWarpSearch: the tile's first row is found by a 32-way warp search
 // (log32 rounds of coalesced loads) instead of lane 0's binary search.
-template <bool kWarpSearch>
+// kUnroll: 32-entry steps handled together by a lane (all neighbour ids of
+// the steps loaded, then all visited probes, then the claims), so more
+// independent loads are in flight.
+template <bool kWarpSearch, int kUnroll>
 __device__ __forceinline__ void td_expand_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -124,23 +153,38 @@ __device__ __forceinline__ void td_expand_body(
     int32_t src = queue[i];
     int64_t rbeg = row_ptr[src];
 #pragma unroll 1
-    for (int k = 0; k < kTdTile / 32; ++k) {
-      const int64_t e = t0 + k * 32 + lane;
-      if (e >= total) break;
-      while (e >= seg_hi && i + 1 < qsize) {
-        ++i;
-        seg_lo = seg_hi;
-        seg_hi = qdeg[i + 1];
-        src = queue[i];
-        rbeg = row_ptr[src];
+    for (int k = 0; k < kTdTile / 32; k += kUnroll) {
+      int32_t us[kUnroll], srcs[kUnroll];
+#pragma unroll
+      for (int j = 0; j < kUnroll; ++j) {
+        const int64_t e = t0 + (k + j) * 32 + lane;
+        us[j] = -1;
+        srcs[j] = 0;
+        if (e < total) {
+          while (e >= seg_hi && i + 1 < qsize) {
+            ++i;
+            seg_lo = seg_hi;
+            seg_hi = qdeg[i + 1];
+            src = queue[i];
+            rbeg = row_ptr[src];
+          }
+          us[j] = __ldg(col + rbeg + (e - seg_lo));
+          srcs[j] = src;
+        }
       }
-      const int32_t u = __ldg(col + rbeg + (e - seg_lo));
-      const uint32_t bit = 1u << (u & 31);
-      // plain load: vis is being updated by this kernel; a stale word only
+      // plain loads: vis is being updated by this kernel; a stale word only
       // causes a redundant (still valid) claim
-      if ((vis[u >> 5] & bit) == 0) {
-        pred[__ldg(inv + u)] = pred_entry(__ldg(inv + src), level);
-        red_or(vis + (u >> 5), bit);
+      uint32_t words[kUnroll];
+#pragma unroll
+      for (int j = 0; j < kUnroll; ++j) words[j] = us[j] >= 0 ? vis[us[j] >> 5] : kFull;
+#pragma unroll
+      for (int j = 0; j < kUnroll; ++j) {
+        if (us[j] < 0) continue;
+        const uint32_t bit = 1u << (us[j] & 31);
+        if ((words[j] & bit) == 0) {
+          pred[__ldg(inv + us[j])] = pred_entry(__ldg(inv + srcs[j]), level);
+          red_or(vis + (us[j] >> 5), bit);
+        }
       }
     }
   }
@@ -662,13 +706,13 @@ __device__ __forceinline__ void frontier_write_body(
 
 // Kernels of the host-driven level loop: thin wrappers around the bodies
 // above, which the device-driven loop (below) shares.
-template <bool kWarpSearch>
+template <bool kWarpSearch, int kUnroll>
 __global__ void __launch_bounds__(256) td_expand_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_expand_body<kWarpSearch>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
+  td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
 }
 
 template <int kWords, int kMinBlocks>
@@ -740,6 +784,7 @@ __global__ void sg_root_kernel(const SgArg* __restrict__ a, const int32_t* __res
                                int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
                                Counters* ctr, SingleCtl* __restrict__ c) {
   const int64_t root = a->root;
+  if (a->prev_root >= 0) pred[a->prev_root] = -1;
   pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
   const int32_t r = rank[root];
   memset(ctr, 0, sizeof(Counters));
@@ -762,6 +807,22 @@ __global__ void sg_root_kernel(const SgArg* __restrict__ a, const int32_t* __res
   c->visited = 1;
   c->qsize = 1;
   for (int i = 0; i < 9; ++i) c->at[i] = a->at[i];
+}
+
+__global__ void sg_reset_unvisited_kernel(const SingleCtl* __restrict__ c,
+                                          uint32_t* const* __restrict__ vis_pp, int64_t W,
+                                          const int32_t* __restrict__ inv,
+                                          int64_t* __restrict__ pred) {
+  const uint32_t* vis = vis_pp[c->cur];
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < W;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t un = ~vis[w];
+    while (un) {
+      const int b = __ffs(un) - 1;
+      un &= un - 1;
+      pred[inv[w * 32 + b]] = -1;
+    }
+  }
 }
 
 // Level start (host loop: ++level, at[8], prev_nq, forward, clear counters).
@@ -797,7 +858,7 @@ __global__ void __launch_bounds__(256) sg_td_kernel(
   if (kForm == 3)
     td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
   else
-    td_expand_body<kForm == 5>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
+    td_expand_body<kForm == 5, 1>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
 }
 
 __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
@@ -951,6 +1012,8 @@ void BfsState::allocate(DeviceArena& arena, const Graph& g) {
   sctl = arena_alloc<SingleCtl>(arena, 1, "search control block");
   sarg = arena_alloc<SgArg>(arena, 1, "search arguments");
   d_vis = arena_alloc<uint32_t*>(arena, 2, "bitmap pointers");
+  pred_clean = false;
+  prev_root = -1;
   check_cuda(cudaMemcpy(d_vis, vis, sizeof(vis), cudaMemcpyHostToDevice), "bitmap pointers");
   check_cuda(cudaMallocHost(&hsctl, sizeof(SingleCtl)), "pinned control block");
   check_cuda(cudaMallocHost(&hsarg, sizeof(SgArg)), "pinned arguments");
@@ -1060,8 +1123,8 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
   st.sgraph = nullptr;
   const Csr& c = g.csr;
   check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
-  init_kernel<<<grid_for(std::max(st.pred_size / 2, st.W), 256, sms, 8), 256, 0, s>>>(
-      st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R);
+  init_kernel<<<grid_for(st.W, 256, sms, 8), 256, 0, s>>>(st.pred, st.pred_size, st.vis[0],
+                                                          st.vis[1], st.W, st.R, 0);
   sg_root_kernel<<<1, 1, 0, s>>>(st.sarg, c.rank, c.row_ptr, st.pred, st.vis[0], st.vis[1],
                                  st.queue, st.qdeg, st.ctr, st.sctl);
   cudaStreamCaptureStatus cs;
@@ -1080,6 +1143,9 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
   if (err == cudaSuccess) err = cudaGraphAddNode(&node, cg, deps, nd, &p);
   if (err == cudaSuccess)
     err = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+  if (err == cudaSuccess)
+    sg_reset_unvisited_kernel<<<grid_for(st.W, 256, sms, 8), 256, 0, s>>>(st.sctl, st.d_vis, st.W,
+                                                                           c.inv, st.pred);
   cudaGraph_t body = err == cudaSuccess ? p.conditional.phGraph_out[0] : nullptr;
   cudaGraph_t outer = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(s, &outer);
@@ -1111,7 +1177,13 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
                         int64_t* at, const RunOptions& opt, b200bfs_run_stats* stats) {
   if (!st.sgexec || st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction))
     sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction);
+  if (!st.pred_clean) {
+    init_kernel<<<grid_for(st.pred_size / 2, 256, sms, 8), 256, 0, s>>>(
+        st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, 1);
+    check_cuda(cudaGetLastError(), "pred fill");
+  }
   SgArg& a = *st.hsarg;
+  a.prev_root = st.pred_clean ? st.prev_root : -1;
   a.root = root;
   a.root_level = root_level;
   a.alpha = alpha;
@@ -1127,6 +1199,8 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   check_cuda(cudaStreamSynchronize(s), "search");
   const SingleCtl& c = *st.hsctl;
   if (c.done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
+  st.pred_clean = true;
+  st.prev_root = root;
   if (at)
     for (int i = 0; i < 9; ++i) at[i] = c.at[i];
   st.levels.clear();
@@ -1146,8 +1220,8 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
     rs.edges_scanned_bu = c.scanned_bu;
     rs.td_bytes = c.td_bytes;
     rs.bu_bytes = c.bu_bytes;
-    rs.algorithmic_bytes = c.bytes + 8 * st.pred_size;
-    rs.kernel_launches = 2 + kSgLevelLaunches * (int)(c.num_td + c.num_bu);
+    rs.algorithmic_bytes = c.bytes + 4 * st.W + 8 * std::max<int64_t>(st.R - c.visited, 0);
+    rs.kernel_launches = 3 + kSgLevelLaunches * (int)(c.num_td + c.num_bu);
     *stats = rs;
   }
 }
@@ -1172,11 +1246,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   // (level kind, event index) of every timed level kernel
   std::vector<std::pair<bool, size_t>> timed;
   size_t nev = 0;
-  init_kernel<<<grid_for(std::max(st.pred_size / 2, st.W), B, sms, 8), B, 0, s>>>(
-      st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R);
-  root_kernel<<<1, 1, 0, s>>>(root, c.rank, c.row_ptr, st.pred, st.vis[0], st.vis[1], st.queue,
-                              st.qdeg, st.ctr);
-  bytes += 8 * st.pred_size;  // pred initialisation
+  const bool fill_pred = !st.pred_clean;
+  init_kernel<<<grid_for(std::max(fill_pred ? st.pred_size / 2 : 0, st.W), B, sms, 8), B, 0, s>>>(
+      st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, fill_pred ? 1 : 0);
+  root_kernel<<<1, 1, 0, s>>>(root, fill_pred ? -1 : st.prev_root, c.rank, c.row_ptr, st.pred,
+                              st.vis[0], st.vis[1], st.queue, st.qdeg, st.ctr);
+  bytes += fill_pred ? 8 * st.pred_size : 4 * st.W;  // pred initialisation / unvisited reset
   int cur = 0;  // vis[cur] is the current visited bitmap
 
   int64_t level = root_level;
@@ -1208,11 +1283,17 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // chunked form once the search has come back from bottom-up (short
       // rows of the tail levels)
       const int td_form = opt.td_kernel == 4 ? (growing ? 5 : 3) : opt.td_kernel;
-      if (td_form == 5)
-        td_expand_kernel<true><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,
-                                                     c.inv, st.vis[cur], st.pred, level);
+      if (td_form == 5 && opt.td_unroll == 4)
+        td_expand_kernel<true, 4><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
+                                                        c.col, c.inv, st.vis[cur], st.pred, level);
+      else if (td_form == 5 && opt.td_unroll == 2)
+        td_expand_kernel<true, 2><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
+                                                        c.col, c.inv, st.vis[cur], st.pred, level);
+      else if (td_form == 5)
+        td_expand_kernel<true, 1><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
+                                                        c.col, c.inv, st.vis[cur], st.pred, level);
       else if (td_form == 1)
-        td_expand_kernel<false><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
+        td_expand_kernel<false, 1><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
                                                st.vis[cur], st.pred, level);
       else if (td_form == 3)
         td_chunk_kernel<<<td_chunk_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,
@@ -1324,6 +1405,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       qsize = global_nq_size;
     }
   }
+  reset_unvisited_kernel<<<grid_for(st.W, B, sms, 8), B, 0, s>>>(st.vis[cur], st.W, c.inv,
+                                                                 st.pred);
+  ++launches;
+  bytes += 8 * std::max<int64_t>(st.R - visited, 0);
+  st.pred_clean = true;
+  st.prev_root = root;
   check_cuda(cudaGetLastError(), "bfs");
   for (size_t k = 0; k < timed.size(); ++k) {
     const auto& t = timed[k];

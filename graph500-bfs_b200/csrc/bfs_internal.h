@@ -24,7 +24,7 @@ struct SgRec {
 };
 // Per-search arguments, written by the host before each graph launch.
 struct SgArg {
-  long long root, root_level;
+  long long root, prev_root, root_level;
   double alpha, beta;
   int edgefactor, want_at;
   long long at[9];
@@ -56,6 +56,11 @@ struct BfsState {
   Counters* hctr = nullptr;               // pinned mirror
   std::vector<cudaEvent_t> ev;            // per-level kernel timing events
   std::vector<b200bfs_level_stats> levels;  // per-level record of the last search
+  // pred holds exactly the last search's result (-1 everywhere else), so the
+  // next search only resets what it leaves unreached; false after
+  // allocation and whenever pred was written by other code.
+  bool pred_clean = false;
+  int64_t prev_root = -1;                 // the last search's root entry
   // device-driven level loop (graph mode)
   SingleCtl* sctl = nullptr;
   SingleCtl* hsctl = nullptr;             // pinned mirror
@@ -83,6 +88,7 @@ struct RunOptions {
   // warp-wide search for each tile's first row.
   int td_kernel = 4;
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
+  int td_unroll = 1;        // td form 5: 32-entry steps per lane handled together (1, 2, 4)
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
   int batch_graph = 1;      // batched search: level loop in a CUDA graph (0: host loop)
   // single-source search: level loop on the device in a CUDA graph (default

@@ -1134,6 +1134,10 @@ void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream
   int hmissing = 0;
   check_cuda(cudaMemcpyAsync(&hmissing, missing, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "batch select");
+  // pred now holds exactly this root's result; its entry vertex is the one
+  // entry outside the rows of the searched graph that a later search resets
+  st.pred_clean = true;
+  st.prev_root = bs.entry_vertex[(size_t)index];
   if (hmissing) throw Error{B200BFS_ERR_CUDA, "batch levels without a parent one level up"};
 }
 

@@ -303,6 +303,7 @@ def test_device_level_loop_matches_host_loop(engine, oracle_graphs, alpha, beta,
     keys = ("levels", "num_td_levels", "num_bu_levels", "bu_level_mask", "visited",
             "edges_scanned_td", "edges_scanned_bu", "algorithmic_bytes", "td_bytes", "bu_bytes")
     try:
+        engine.run(int(roots[0]), 16, alpha, beta)  # the first search fills pred once
         for r in roots:
             r = int(r)
             engine.set_option("single_graph", 0)
@@ -323,6 +324,46 @@ def test_device_level_loop_matches_host_loop(engine, oracle_graphs, alpha, beta,
         if not flags:
             engine.set_option("single_graph", 1)
             _check_search(engine, edges, g, roots, alpha, beta)
+    finally:
+        engine.set_option("single_graph", 0)
+        engine.end()
+
+
+@pytest.mark.parametrize("single_graph", [0, 1])
+def test_pred_exact_across_searches(engine, oracle_graphs, single_graph):
+    """pred is not refilled with -1 before every search: each search resets
+    the rows it leaves unreached and the previous root's entry.  Searches
+    that reach different vertex sets (giant component, a small component, an
+    isolated vertex, a batch result in between) must each leave exactly
+    their own result."""
+    edges, g = oracle_graphs(16)
+    engine.generate_graph(16, 16)
+    engine.prepare(16)
+    he = g.has_edge()
+    big = [int(r) for r in O.find_roots(he, 1 << 16, 2)]
+    small = None
+    for v in np.nonzero(he)[0][::-1]:
+        lv = g.levels(int(v))
+        if 1 < int((lv >= 0).sum()) < 1000:
+            small = int(v)
+            break
+    assert small is not None
+    isolated = int(np.nonzero(he == 0)[0][0])
+    try:
+        engine.set_option("single_graph", single_graph)
+        for r in [big[0], small, big[1], isolated, small, big[0]]:
+            engine.run(r)
+            assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r)), r
+            assert np.all(engine.get_pred()[g.nverts:] == -1)
+            err, _ = engine.validate(r)
+            assert err == 0, r
+        engine.run_batch([small, big[1]])
+        engine.batch_select(0)
+        engine.run(big[0])
+        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(big[0]))
+        engine.batch_select(1)
+        engine.run(small)
+        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(small))
     finally:
         engine.set_option("single_graph", 0)
         engine.end()
