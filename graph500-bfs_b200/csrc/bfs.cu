@@ -274,12 +274,16 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
 // probes, back to back: kWords * 2 independent loads are in flight per lane
 // instead of one dependent chain.  Rows unresolved after 8 probes are swept
 // by the whole warp as in bu_kernel.
-template <int kWords>
+// kFirst: each open row first probes its first neighbour from the dense
+// first[] array (one coalesced read for the warp), and loads its row offsets
+// only when that probe misses; the offset rounds then start at the second
+// neighbour.
+template <int kWords, bool kFirst>
 __device__ __forceinline__ void bu_wide_body(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ inv, int64_t* __restrict__ pred, int64_t level,
-    Counters* __restrict__ ctr) {
+    const int32_t* __restrict__ first, const int32_t* __restrict__ inv,
+    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -298,14 +302,40 @@ __device__ __forceinline__ void bu_wide_body(
     }
     int64_t b[kWords], e[kWords];
     int32_t par[kWords];
+    if (kFirst) {
+      int32_t f[kWords];
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      par[k] = -1;
-      b[k] = e[k] = 0;
-      if (((~c[k]) >> lane) & 1u) {
-        const int64_t v = (w0 + k) * 32 + lane;
-        b[k] = row_ptr[v];
-        e[k] = row_ptr[v + 1];
+      for (int k = 0; k < kWords; ++k) {
+        par[k] = -1;
+        b[k] = e[k] = 0;
+        f[k] = -1;
+        if (((~c[k]) >> lane) & 1u) f[k] = __ldg(first + (w0 + k) * 32 + lane);
+      }
+      uint32_t mf[kWords];
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) mf[k] = f[k] >= 0 ? __ldg(cur + (f[k] >> 5)) : 0u;
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) {
+        if (f[k] < 0) continue;
+        scanned += 1;
+        if ((mf[k] >> (f[k] & 31)) & 1u) {
+          par[k] = f[k];
+        } else {
+          const int64_t v = (w0 + k) * 32 + lane;
+          b[k] = row_ptr[v] + 1;
+          e[k] = row_ptr[v + 1];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kWords; ++k) {
+        par[k] = -1;
+        b[k] = e[k] = 0;
+        if (((~c[k]) >> lane) & 1u) {
+          const int64_t v = (w0 + k) * 32 + lane;
+          b[k] = row_ptr[v];
+          e[k] = row_ptr[v + 1];
+        }
       }
     }
     // four rounds of two probes per vertex
@@ -715,13 +745,13 @@ __global__ void __launch_bounds__(256) td_expand_kernel(
   td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
 }
 
-template <int kWords, int kMinBlocks>
+template <int kWords, int kMinBlocks, bool kFirst>
 __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ inv, int64_t* __restrict__ pred, int64_t level,
-    Counters* __restrict__ ctr) {
-  bu_wide_body<kWords>(cur, nxt, W, row_ptr, col, inv, pred, level, ctr);
+    const int32_t* __restrict__ first, const int32_t* __restrict__ inv,
+    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
+  bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, inv, pred, level, ctr);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
@@ -861,14 +891,16 @@ __global__ void __launch_bounds__(256) sg_td_kernel(
     td_expand_body<kForm == 5, 1>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
 }
 
+template <bool kFirst>
 __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
     const SingleCtl* __restrict__ c, int64_t W, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
-    uint32_t* const* __restrict__ vis_pp, int64_t* __restrict__ pred,
-    Counters* __restrict__ ctr) {
+    const int32_t* __restrict__ col, const int32_t* __restrict__ first,
+    const int32_t* __restrict__ inv, uint32_t* const* __restrict__ vis_pp,
+    int64_t* __restrict__ pred, Counters* __restrict__ ctr) {
   if (c->done || c->forward) return;
   const int cur = c->cur;
-  bu_wide_body<4>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, inv, pred, c->level, ctr);
+  bu_wide_body<4, kFirst>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, inv, pred,
+                          c->level, ctr);
 }
 
 // kAfterBu = false: after a top-down level; true: after a bottom-up level
@@ -1075,7 +1107,7 @@ int chunk_blocks_per_sm() {
 
 // One level of the device-driven loop (captured into the WHILE body).
 void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
-                     int force_direction, cudaGraphConditionalHandle cond) {
+                     int force_direction, bool bu_first, cudaGraphConditionalHandle cond) {
   const Csr& c = g.csr;
   const int B = 256;
   const unsigned nblk = (unsigned)st.nblk;
@@ -1087,8 +1119,12 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
   sg_td_kernel<3><<<sms * chunk_blocks_per_sm(), B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg,
                                                              st.ctr, c.row_ptr, c.col, c.inv,
                                                              st.d_vis, st.pred);
-  sg_bu_kernel<<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.inv, st.d_vis, st.pred,
-                                     st.ctr);
+  if (bu_first && c.first)
+    sg_bu_kernel<true><<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.first, c.inv,
+                                             st.d_vis, st.pred, st.ctr);
+  else
+    sg_bu_kernel<false><<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.first, c.inv,
+                                              st.d_vis, st.pred, st.ctr);
   sg_count_kernel<false><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                          c.row_ptr, c.mdeg, st.blk_cnt,
                                                          st.blk_deg, st.ctr);
@@ -1104,19 +1140,19 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
 constexpr int kSgLevelLaunches = 11;
 
 std::vector<const void*> sg_key(const Graph& g, const BfsState& st, int sms, int td_form,
-                                int force_direction) {
+                                int force_direction, bool bu_first) {
   const Csr& c = g.csr;
   return {st.sctl, st.sarg, st.d_vis, st.ctr, st.fr, st.queue, st.qdeg, st.blk_cnt, st.blk_deg,
           st.pred, st.vis[0], st.vis[1], c.row_ptr, c.col, c.inv, c.rank, c.mdeg,
           (const void*)(intptr_t)st.W, (const void*)(intptr_t)st.R,
           (const void*)(intptr_t)st.pred_size, (const void*)(intptr_t)c.nedges,
           (const void*)(intptr_t)sms, (const void*)(intptr_t)td_form,
-          (const void*)(intptr_t)force_direction};
+          (const void*)(intptr_t)force_direction, c.first, (const void*)(intptr_t)bu_first};
 }
 
 // [init, root] then WHILE(level); the control kernel sets the condition.
 void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
-                    int force_direction) {
+                    int force_direction, bool bu_first) {
   if (st.sgexec) cudaGraphExecDestroy(st.sgexec);
   if (st.sgraph) cudaGraphDestroy(st.sgraph);
   st.sgexec = nullptr;
@@ -1155,7 +1191,7 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
     err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
-      sg_launch_level(g, st, s, sms, td_form, force_direction, cond);
+      sg_launch_level(g, st, s, sms, td_form, force_direction, bu_first, cond);
       cudaGraph_t b2 = nullptr;
       err = cudaStreamEndCapture(s, &b2);
     }
@@ -1168,16 +1204,19 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
     cudaGetLastError();
     check_cuda(err, "search level-loop graph");
   }
-  st.skey = sg_key(g, st, sms, td_form, force_direction);
+  st.skey = sg_key(g, st, sms, td_form, force_direction, bu_first);
 }
 
 // run_bfs_core with the level loop on the device.
 void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                         int64_t root_level, int edgefactor, double alpha, double beta,
                         int64_t* at, const RunOptions& opt, b200bfs_run_stats* stats) {
-  if (!st.sgexec || st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction))
-    sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction);
+  const bool bu_first = opt.bu_first != 0;
+  if (!st.sgexec ||
+      st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction, bu_first))
+    sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction, bu_first);
   if (!st.pred_clean) {
+    st.tree_clean = false;
     init_kernel<<<grid_for(st.pred_size / 2, 256, sms, 8), 256, 0, s>>>(
         st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, 1);
     check_cuda(cudaGetLastError(), "pred fill");
@@ -1247,6 +1286,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   std::vector<std::pair<bool, size_t>> timed;
   size_t nev = 0;
   const bool fill_pred = !st.pred_clean;
+  if (fill_pred) st.tree_clean = false;
   init_kernel<<<grid_for(std::max(fill_pred ? st.pred_size / 2 : 0, st.W), B, sms, 8), B, 0, s>>>(
       st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, fill_pred ? 1 : 0);
   root_kernel<<<1, 1, 0, s>>>(root, fill_pred ? -1 : st.prev_root, c.rank, c.row_ptr, st.pred,
@@ -1311,15 +1351,21 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       ++rs.num_bu_levels;
       if (level < 64) rs.bu_level_mask |= 1ull << level;
       if (opt.bu_kernel == 2)
-        bu_wide_kernel<2, 8><<<bu_wide_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
-                                                        c.row_ptr, c.col, c.inv, st.pred, level,
-                                                        st.ctr);
+        bu_wide_kernel<2, 8, false><<<bu_wide_grid, B, 0, s>>>(
+            st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first, c.inv, st.pred, level,
+            st.ctr);
       else if (opt.bu_kernel == 3)
-        bu_wide_kernel<2, 6><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr,
-                                                   c.col, c.inv, st.pred, level, st.ctr);
+        bu_wide_kernel<2, 6, false><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
+                                                          c.row_ptr, c.col, c.first, c.inv,
+                                                          st.pred, level, st.ctr);
+      else if (opt.bu_kernel == 4 && opt.bu_first && c.first)
+        bu_wide_kernel<4, 4, true><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
+                                                         c.row_ptr, c.col, c.first, c.inv,
+                                                         st.pred, level, st.ctr);
       else if (opt.bu_kernel == 4)
-        bu_wide_kernel<4, 4><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr,
-                                                   c.col, c.inv, st.pred, level, st.ctr);
+        bu_wide_kernel<4, 4, false><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
+                                                          c.row_ptr, c.col, c.first, c.inv,
+                                                          st.pred, level, st.ctr);
       else if (opt.bu_probe <= 4)
         bu_kernel<4><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
                                            c.inv, st.pred, level, st.ctr);

@@ -61,6 +61,10 @@ struct BfsState {
   // allocation and whenever pred was written by other code.
   bool pred_clean = false;
   int64_t prev_root = -1;                 // the last search's root entry
+  // CoreBFS: pred holds the tree parents (level 0xFFFF) of all pruned
+  // vertices except the last climb, whose vertices carry their levels.
+  bool tree_clean = false;
+  std::vector<int64_t> prev_path_v;
   // device-driven level loop (graph mode)
   SingleCtl* sctl = nullptr;
   SingleCtl* hsctl = nullptr;             // pinned mirror
@@ -88,6 +92,7 @@ struct RunOptions {
   // warp-wide search for each tile's first row.
   int td_kernel = 4;
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
+  int bu_first = 1;         // bottom-up form 4: probe the dense first-neighbour array first
   int td_unroll = 1;        // td form 5: 32-entry steps per lane handled together (1, 2, 4)
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
   int batch_graph = 1;      // batched search: level loop in a CUDA graph (0: host loop)

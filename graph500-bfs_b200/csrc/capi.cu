@@ -526,6 +526,9 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "td_kernel") {
       require(value >= 1 && value <= 5, B200BFS_ERR_INVALID, "td_kernel must be 1..5");
       e.opt.td_kernel = (int)value;
+    } else if (n == "bu_first") {
+      require(value == 0 || value == 1, B200BFS_ERR_INVALID, "bu_first must be 0 or 1");
+      e.opt.bu_first = (int)value;
     } else if (n == "td_unroll") {
       require(value == 1 || value == 2 || value == 4, B200BFS_ERR_INVALID,
               "td_unroll must be 1, 2 or 4");

@@ -177,6 +177,13 @@ __global__ void compact_rows_kernel(const int32_t* __restrict__ raw,
   }
 }
 
+__global__ void first_kernel(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                             int64_t R, int32_t* __restrict__ first) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < R;
+       r += (int64_t)gridDim.x * blockDim.x)
+    first[r] = row_ptr[r + 1] > row_ptr[r] ? col[row_ptr[r]] : -1;
+}
+
 __global__ void max_degree_kernel(const int64_t* __restrict__ row_ptr, int64_t R,
                                   unsigned long long* out) {
   unsigned long long acc = 0;
@@ -399,7 +406,15 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   arena.free(len64);
   arena.free(d_u64);
   if (row_of_key) arena.free(row_of_key);
+  build_first(arena, s, c, sms);
   check_cuda(cudaGetLastError(), "build_csr");
+}
+
+void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms) {
+  arena.free(c.first);
+  c.first = arena_alloc<int32_t>(arena, c.nrows, "first neighbours");
+  first_kernel<<<grid_for(c.nrows, 256, sms, 16), 256, 0, s>>>(c.row_ptr, c.col, c.nrows, c.first);
+  check_cuda(cudaGetLastError(), "first neighbours");
 }
 
 }  // namespace b200bfs

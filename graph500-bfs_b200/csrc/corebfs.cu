@@ -381,7 +381,9 @@ void build_core(DeviceArena& arena, cudaStream_t s, Graph& g, int sms) {
   arena.free(c.inv);
   arena.free(c.rank);
   arena.free(c.mdeg);
+  arena.free(c.first);
   c = k2;
+  build_first(arena, s, c, sms);
   k.enabled = true;
   k.core_vertices = Rc;
   rebuild_tree_list(arena, s, sms, g);
@@ -467,6 +469,17 @@ int core_write_tree(const Graph& g, int64_t* pred, const std::vector<int64_t>& p
   return (nt > 0 ? 1 : 0) + 1;
 }
 
+constexpr int kMaxRewrite = 2 * kMaxPath;
+struct RewriteArg {
+  int n;
+  int64_t v[kMaxRewrite];
+  int64_t e[kMaxRewrite];
+};
+
+__global__ void rewrite_kernel(RewriteArg a, int64_t* __restrict__ pred) {
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) pred[a.v[i]] = a.e[i];
+}
+
 void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                   int edgefactor, double alpha, double beta, int64_t* at, const RunOptions& opt,
                   b200bfs_run_stats* stats) {
@@ -474,9 +487,39 @@ void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   int64_t u = root, lv = 0;
   core_climb(g, root, pv, pe, &u, &lv);
   run_bfs_core(g, st, s, sms, u, lv, edgefactor, alpha, beta, at, opt, stats);
-  const int launches = core_write_tree(g, st.pred, pv, pe, s, sms);
+  int launches;
+  int64_t bytes;
+  if (!st.tree_clean) {
+    // write_tree_parents (corebfs_adaptor.hpp:285-301): every pruned vertex
+    launches = core_write_tree(g, st.pred, pv, pe, s, sms);
+    bytes = 16 * g.core.tree_vertices;
+    st.tree_clean = true;
+  } else {
+    // pred already holds every tree parent with level 0xFFFF except on the
+    // previous climb: put those back (unless on this climb), then this climb
+    RewriteArg a;
+    a.n = 0;
+    const std::vector<int32_t>& tp = g.core.h_tree_parent;
+    for (int64_t v : st.prev_path_v) {
+      if (tp[(size_t)v] < 0) continue;  // the core entry: handled by the search
+      if (std::find(pv.begin(), pv.end(), v) != pv.end()) continue;
+      a.v[a.n] = v;
+      a.e[a.n] = pred_entry(tp[(size_t)v], 0xFFFF);
+      ++a.n;
+    }
+    for (size_t i = 0; i < pv.size(); ++i) {
+      a.v[a.n] = pv[i];
+      a.e[a.n] = pe[i];
+      ++a.n;
+    }
+    rewrite_kernel<<<1, 128, 0, s>>>(a, st.pred);
+    check_cuda(cudaGetLastError(), "core climb");
+    launches = 1;
+    bytes = 16 * a.n;
+  }
+  st.prev_path_v = pv;
   if (stats) {
-    stats->algorithmic_bytes += 16 * g.core.tree_vertices;
+    stats->algorithmic_bytes += bytes;
     stats->kernel_launches += launches;
   }
 }

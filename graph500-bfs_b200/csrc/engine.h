@@ -86,6 +86,11 @@ struct Csr {
   int32_t* inv = nullptr;      // [R]     row -> original id
   int32_t* rank = nullptr;     // [nverts] original id -> row, -1 if no edge
   int32_t* mdeg = nullptr;     // [R]     pre-dedup degree (degree_, graph_constructor.hpp:572-592)
+  // [R] first (highest-degree) neighbour of each row, kept apart so that a
+  // bottom-up probe of it is one coalesced 4-byte read per row (the
+  // reference keeps each row's first edge apart too: isolated_edges_,
+  // graph_constructor.hpp:1224-1348)
+  int32_t* first = nullptr;
   int64_t max_degree = 0;
 };
 
@@ -119,6 +124,9 @@ struct Graph {
   bool input_symmetric = false;
   int64_t device_bytes = 0;
 };
+
+// Fills c.first from c.row_ptr and c.col.
+void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms);
 
 // Builds g.csr from nedges device edges (each a (v0, v1) pair of uint32 ids).
 void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t nedges,

@@ -36,6 +36,7 @@ struct Engine {
     arena.free(g.csr.inv);
     arena.free(g.csr.rank);
     arena.free(g.csr.mdeg);
+    arena.free(g.csr.first);
     arena.free(g.input_edges);
     g = Graph();
   }

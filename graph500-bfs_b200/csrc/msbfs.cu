@@ -1138,6 +1138,10 @@ void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream
   // entry outside the rows of the searched graph that a later search resets
   st.pred_clean = true;
   st.prev_root = bs.entry_vertex[(size_t)index];
+  if (g.core.enabled) {
+    st.tree_clean = true;  // core_write_tree wrote every tree parent
+    st.prev_path_v = bs.path_v[(size_t)index];
+  }
   if (hmissing) throw Error{B200BFS_ERR_CUDA, "batch levels without a parent one level up"};
 }
 
