@@ -1350,15 +1350,24 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     } else {
       ++rs.num_bu_levels;
       if (level < 64) rs.bu_level_mask |= 1ull << level;
-      if (opt.bu_kernel == 2)
+      const bool first = opt.bu_first && c.first;
+      if (opt.bu_kernel == 2 && first)
+        bu_wide_kernel<2, 8, true><<<bu_wide_grid, B, 0, s>>>(
+            st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first, c.inv, st.pred, level,
+            st.ctr);
+      else if (opt.bu_kernel == 2)
         bu_wide_kernel<2, 8, false><<<bu_wide_grid, B, 0, s>>>(
             st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first, c.inv, st.pred, level,
             st.ctr);
+      else if (opt.bu_kernel == 3 && first)
+        bu_wide_kernel<2, 6, true><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
+                                                         c.row_ptr, c.col, c.first, c.inv,
+                                                         st.pred, level, st.ctr);
       else if (opt.bu_kernel == 3)
         bu_wide_kernel<2, 6, false><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
                                                           c.row_ptr, c.col, c.first, c.inv,
                                                           st.pred, level, st.ctr);
-      else if (opt.bu_kernel == 4 && opt.bu_first && c.first)
+      else if (opt.bu_kernel == 4 && first)
         bu_wide_kernel<4, 4, true><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
                                                          c.row_ptr, c.col, c.first, c.inv,
                                                          st.pred, level, st.ctr);

@@ -309,10 +309,14 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // atomics.  The frontier masks of level L-1 are
 // only read here, and a bit of U can only come from a neighbour at level
 // L-1 of that root, so the OR over neighbours is exact.
+// first (may be null): the rows' first neighbours; an open row ORs its first
+// neighbour's mask (one coalesced read of first[] per warp) before loading
+// its row offsets, which it then needs only if that mask does not cover U.
 template <int kProbe>
 __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ctl,
                                                        const int64_t* __restrict__ row_ptr,
-                                                       const int32_t* __restrict__ col) {
+                                                       const int32_t* __restrict__ col,
+                                                       const int32_t* __restrict__ first) {
   if (!ctl->has_bu) return;
   const long long L = ctl->level;
   const int64_t R = ctl->R;
@@ -339,7 +343,16 @@ __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ct
     rows += (lane == 0) ? __popc(work) : 0;
     unsigned long long acc = 0;
     int64_t j = 0, e = 0;
-    if (U) {
+    if (first) {
+      if (U) {
+        acc = __ldg(prev + __ldg(first + v));
+        scanned += 1;
+        if ((acc & U) != U) {
+          j = row_ptr[v] + 1;
+          e = row_ptr[v + 1];
+        }
+      }
+    } else if (U) {
       j = row_ptr[v];
       e = row_ptr[v + 1];
     }
@@ -761,6 +774,7 @@ void ensure_batch_view(DeviceArena& arena, Graph& g, cudaStream_t s, int sms) {
   v.col = arena_alloc<int32_t>(arena, c.nedges, "view adjacency");
   bview_copy_kernel<<<grid_for(R * 32, B, sms, 8), B, 0, s>>>(order, R, c.row_ptr, c.col,
                                                                g.b_of_row, v.row_ptr, v.col);
+  build_first(arena, s, v, sms);
   check_cuda(cudaStreamSynchronize(s), "batch view");
   arena.free(order);
   g.bview = v;
@@ -773,6 +787,7 @@ void free_batch_view(DeviceArena& arena, Graph& g) {
   arena.free(g.bview.col);
   arena.free(g.bview.inv);
   arena.free(g.bview.mdeg);
+  arena.free(g.bview.first);
   arena.free(g.b_of_row);
   g.bview = Csr();
   g.b_of_row = nullptr;
@@ -890,7 +905,7 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
   batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
                                                       bs.queue, bs.qdeg);
   if (ev) check_cuda(cudaEventRecord(ev[1], s), "event");
-  batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col);
+  batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
   batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg, c.row_ptr, c.col);
   if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
@@ -909,7 +924,7 @@ void launch_prologue(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
 std::vector<const void*> graph_key_of(const Graph& g, const BatchState& bs, int sms) {
   const Csr& c = batch_csr(g);
   return {bs.ctl, bs.d_arg, bs.blk_cnt, bs.blk_deg, (const void*)(intptr_t)bs.nblk,
-          (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, g.csr.rank, g.b_of_row,
+          (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, c.first, g.csr.rank, g.b_of_row,
           (const void*)(intptr_t)g.nverts, bs.queue, bs.qdeg, (const void*)(intptr_t)sms};
 }
 
