@@ -588,6 +588,11 @@ __device__ __forceinline__ void td_chunk_body(
 
 // Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
 // vertices, their CSR degrees and their pre-dedup degrees.
+// kDeg: also the per-block CSR degree sums of the frontier, which only a
+// following top-down level needs (its queue's degree prefix); after a
+// top-down level they are computed by frontier_deg_body once the next
+// direction is known.
+template <bool kDeg>
 __device__ __forceinline__ void frontier_count_body(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
@@ -605,7 +610,7 @@ __device__ __forceinline__ void frontier_count_body(
       const int bpos = __ffs(f) - 1;
       f &= f - 1;
       const int64_t v = w * 32 + bpos;
-      dsum += row_ptr[v + 1] - row_ptr[v];
+      if (kDeg) dsum += row_ptr[v + 1] - row_ptr[v];
       msum += mdeg[v];
     }
   }
@@ -630,11 +635,37 @@ __device__ __forceinline__ void frontier_count_body(
       C += s_c[i];
     }
     blk_cnt[blockIdx.x] = A;
-    blk_deg[blockIdx.x] = Bs;
+    if (kDeg) blk_deg[blockIdx.x] = Bs;
     if (A) {
       atomicAdd(&ctr->nq, (unsigned long long)A);
       atomicAdd(&ctr->nq_edges, (unsigned long long)C);
     }
+  }
+}
+
+// Per-block CSR degree sums of the frontier bitmap fr.
+__device__ __forceinline__ void frontier_deg_body(const uint32_t* __restrict__ fr, int64_t W,
+                                                  const int64_t* __restrict__ row_ptr,
+                                                  int64_t* __restrict__ blk_deg) {
+  __shared__ int64_t s_b[kWordsPerBlock / 32];
+  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
+  int64_t dsum = 0;
+  if (w < W) {
+    uint32_t f = fr[w];
+    while (f) {
+      const int64_t v = w * 32 + __ffs(f) - 1;
+      f &= f - 1;
+      dsum += row_ptr[v + 1] - row_ptr[v];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) dsum += __shfl_xor_sync(kFull, dsum, o);
+  if (lane_id() == 0) s_b[threadIdx.x >> 5] = dsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t b = 0;
+    for (int i = 0; i < kWordsPerBlock / 32; ++i) b += s_b[i];
+    blk_deg[blockIdx.x] = b;
   }
 }
 
@@ -762,11 +793,18 @@ __global__ void __launch_bounds__(256) td_chunk_kernel(
   td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
 }
 
+template <bool kDeg>
 __global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
     int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
-  frontier_count_body(nw, old, fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+  frontier_count_body<kDeg>(nw, old, fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+}
+
+__global__ void __launch_bounds__(kWordsPerBlock) frontier_deg_kernel(
+    const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
+    int64_t* __restrict__ blk_deg) {
+  frontier_deg_body(fr, W, row_ptr, blk_deg);
 }
 
 __global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict__ blk_cnt,
@@ -914,7 +952,17 @@ __global__ void __launch_bounds__(kWordsPerBlock) sg_count_kernel(
   if (c->done) return;
   if (kAfterBu ? (c->forward || !c->next_forward) : !c->forward) return;
   const int cur = c->cur;
-  frontier_count_body(vis_pp[cur], vis_pp[cur ^ 1], fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+  frontier_count_body<kAfterBu>(vis_pp[cur], vis_pp[cur ^ 1], fr, W, row_ptr, mdeg, blk_cnt,
+                                blk_deg, ctr);
+}
+
+// After a top-down level whose next level is top-down: the queue's degree
+// sums.
+__global__ void __launch_bounds__(kWordsPerBlock) sg_deg_kernel(
+    const SingleCtl* __restrict__ c, const uint32_t* __restrict__ fr, int64_t W,
+    const int64_t* __restrict__ row_ptr, int64_t* __restrict__ blk_deg) {
+  if (c->done || !c->forward || !c->next_forward) return;
+  frontier_deg_body(fr, W, row_ptr, blk_deg);
 }
 
 __global__ void __launch_bounds__(1024) sg_scan_kernel(const SingleCtl* __restrict__ c,
@@ -1133,11 +1181,12 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
   sg_count_kernel<true><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                         c.row_ptr, c.mdeg, st.blk_cnt,
                                                         st.blk_deg, st.ctr);
+  sg_deg_kernel<<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_deg);
   sg_scan_kernel<<<1, 1024, 0, s>>>(st.sctl, st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
   sg_write_kernel<<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_cnt,
                                                   st.blk_deg, st.queue, st.qdeg);
 }
-constexpr int kSgLevelLaunches = 11;
+constexpr int kSgLevelLaunches = 12;
 
 std::vector<const void*> sg_key(const Graph& g, const BfsState& st, int sms, int td_form,
                                 int force_direction, bool bu_first) {
@@ -1343,7 +1392,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
                                              st.vis[cur], st.pred, level);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 2;
-      frontier_count_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+      frontier_count_kernel<false><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
           st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
           st.ctr);
       frontier_in = qsize;
@@ -1450,13 +1499,16 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     if (next_forward) {
       // Build the next queue from the bits set in this level.
       if (!forward)  // after bottom-up: bits of vis[cur] not in vis[cur^1]
-        frontier_count_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+        frontier_count_kernel<true><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
             st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
             st.ctr);
+      else  // after top-down: the counts are there, the degree sums not yet
+        frontier_deg_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(st.fr, st.W, c.row_ptr,
+                                                                         st.blk_deg);
       frontier_scan_kernel<<<1, 1024, 0, s>>>(st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
       frontier_write_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
           st.fr, st.W, c.row_ptr, st.blk_cnt, st.blk_deg, st.queue, st.qdeg);
-      launches += forward ? 2 : 3;
+      launches += 3;
       qsize = global_nq_size;
     }
   }
