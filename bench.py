@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
                    help="alpha of the batched search (<= 0: the engine's batch default)")
+    p.add_argument("--batch-sweep", action="store_true",
+                   help="also time batches of 1, 8, 32 and 64 roots")
     p.add_argument("--batch-host-loop", action="store_true",
                    help="batched search with the host-driven level loop (for profilers that "
                         "cannot see kernels inside conditional CUDA graphs)")
@@ -318,6 +320,23 @@ def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
     err, cnt = eng.validate(r_last)
     if err != 0 or cnt != nedge[idx[r_last]]:
         raise RuntimeError(f"batched result for root {r_last} failed validation")
+    sweep = []
+    if args.batch_sweep:
+        for kk in (1, 8, 32, 64):
+            kk = min(kk, len(roots))
+            ts = []
+            for b in range(6):
+                sub = np.roll(roots, 5 * b)[:kk]
+                a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                eng.run_batch(sub, args.edgefactor, args.batch_alpha, args.beta)
+                e.record(stream)
+                e.synchronize()
+                if b:  # the first is a warm-up
+                    ts.append(a.elapsed_time(e) / 1e3)
+            tk = barrier_max(dist, float(np.median(ts)))
+            sweep.append({"roots_per_batch": kk, "batch_ms": 1e3 * tk,
+                          "bfs_per_s": (dist.get_world_size() if dist else 1) * kk / tk})
     t_batch = barrier_max(dist, float(np.median(times)))
     t_single = barrier_max(dist, float(np.mean(single_times)))
     world = dist.get_world_size() if dist is not None else 1
@@ -338,6 +357,7 @@ def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
         / max(1.0, float(eng.info().num_input_edges)),
         "algorithmic_gbs": stats.algorithmic_bytes / (stats.ms / 1e3) / 1e9,
         "level_loop": "CUDA graph (WHILE conditional node), one host sync per batch",
+        "sweep": sweep or None,
     }
 
 
