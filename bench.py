@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
                    help="alpha of the batched search (<= 0: the engine's batch default)")
+    p.add_argument("--engine-option", action="append", default=[], metavar="NAME=VALUE",
+                   help="set an engine option (b200bfs_set_option) before timing; repeatable")
     p.add_argument("--batch-sweep", action="store_true",
                    help="also time batches of 1, 8, 32 and 64 roots")
     p.add_argument("--batch-host-loop", action="store_true",
@@ -509,6 +511,9 @@ def main():
                                                  args.beta)
         log(f"[rank {rank}] -A tuning: alpha {args.alpha:.4g}, beta {args.beta:.4g} "
             f"({time.time() - t0:.1f}s)")
+    for kv in args.engine_option:
+        name, value = kv.split("=", 1)
+        eng.set_option(name, int(value))
     tuner = None
     if args.tune_engine:
         t0 = time.time()
