@@ -591,6 +591,18 @@ def main():
                     kms / (1e3 * sum(times)) if times else None,
                 "whole_search_algorithmic_gbs":
                     sum(s.algorithmic_bytes for s in stats) / sum(times) / 1e9}
+    # every kernel group of the search against the same peak
+    pred_ms = sum(s.pred_ms for s in stats)
+    kernels = {}
+    for name, ms, nbytes in (("bu_wide_kernel", bu_ms, sum(s.bu_bytes for s in stats)),
+                             ("td_expand_kernel", td_ms, sum(s.td_bytes for s in stats)),
+                             ("assemble_pred_kernel", pred_ms,
+                              sum(s.pred_bytes for s in stats))):
+        if ms > 0:
+            gbs = nbytes / (ms / 1e3) / 1e9
+            kernels[name] = {"ms_per_search": ms / len(stats), "achieved_gbs": gbs,
+                             "frac": gbs / peak,
+                             "share_of_search_time": ms / (1e3 * sum(times))}
 
     line = {
         "metric": f"harmonic-mean GTEPS, SCALE {args.scale}; 64-root batched BFS/s + p99 vs 1-root",
@@ -603,6 +615,7 @@ def main():
         "e2e": {"value": e2e, "unit": "GTEPS", "h2d_bytes_per_step": 8,
                 "d2h_bytes_per_step": 8 * info.pred_size},
         "roofline": roofline,
+        "kernels": kernels,
         "clocks": clk,
         "gpu_launches": int(barrier_sum(dist, sum(s.kernel_launches for s in stats))),
         "batched": batched,
@@ -612,6 +625,7 @@ def main():
                        / (info.num_input_edges or 1),
                    "levels": int(np.median([s.levels for s in stats])),
                    "td_ms": td_ms / args.steps, "bu_ms": bu_ms / args.steps,
+                   "pred_ms": pred_ms / args.steps,
                    "build_s": t_build},
     }
     eng.end()

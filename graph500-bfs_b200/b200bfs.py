@@ -78,7 +78,8 @@ class RunStats(ctypes.Structure):
                 ("edges_scanned_td", ctypes.c_int64), ("edges_scanned_bu", ctypes.c_int64),
                 ("algorithmic_bytes", ctypes.c_int64), ("td_bytes", ctypes.c_int64),
                 ("bu_bytes", ctypes.c_int64), ("device_ms", ctypes.c_double),
-                ("td_ms", ctypes.c_double), ("bu_ms", ctypes.c_double)]
+                ("td_ms", ctypes.c_double), ("bu_ms", ctypes.c_double),
+                ("pred_bytes", ctypes.c_int64), ("pred_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -69,14 +69,20 @@ __global__ void init_kernel(int64_t* __restrict__ pred, int64_t pred_size,
 
 // prev_root: the previous search's root entry, cleared first (it is not
 // covered by the reset of unvisited rows when it is not a row of the CSR).
+// row_mode: pred is the row-order buffer of the assembly pass; the root's
+// row gets the root entry there (an edgeless root gets it in the assembly).
 __global__ void root_kernel(int64_t root, int64_t prev_root, const int32_t* __restrict__ rank,
                             const int64_t* __restrict__ row_ptr, int64_t* __restrict__ pred,
                             uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1,
                             int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
-                            Counters* ctr) {
-  if (prev_root >= 0) pred[prev_root] = -1;
-  pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
+                            Counters* ctr, int row_mode) {
   int32_t r = rank[root];
+  if (row_mode) {
+    if (r >= 0) pred[r] = root;
+  } else {
+    if (prev_root >= 0) pred[prev_root] = -1;
+    pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
+  }
   memset(ctr, 0, sizeof(Counters));
   if (r >= 0) {
     vis0[r >> 5] |= 1u << (r & 31);
@@ -111,6 +117,72 @@ __global__ void reset_unvisited_kernel(const uint32_t* __restrict__ vis, int64_t
   }
 }
 
+// Assembly of pred from the row-order buffer rp (engine option
+// pred_assemble).  pmap[u] for original id u: its row (>= 0), -1 (no parent:
+// no edge, or beyond the graph), or -(p + 2) for a CoreBFS pruned vertex with
+// tree parent p.  A reached row gives its rp entry, an unreached row -1, a
+// pruned vertex its tree entry (level 0xFFFF, as write_tree_kernel writes),
+// the root itself.  The pass runs over u in order, so pred is written in full
+// lines; with group reordering the rows of a group of 2^16 ids are
+// contiguous, so the rp reads of the ids a wave of warps covers fall in a few
+// windows that stay in L2.  Scattering the entries by original id during the
+// levels instead costs a random 32-byte sector per entry.
+__device__ __forceinline__ int64_t assembled_entry(int32_t m, int64_t u,
+                                                   const uint32_t* __restrict__ vis,
+                                                   const int64_t* __restrict__ rp, int64_t root) {
+  int64_t e = -1;
+  if (m >= 0) {
+    if ((__ldg(vis + (m >> 5)) >> (m & 31)) & 1u) e = __ldg(rp + m);
+  } else if (m < -1) {
+    e = pred_entry(-(int64_t)m - 2, 0xFFFF);
+  }
+  return u == root ? root : e;
+}
+
+// Four ids per thread: one 16-byte map load, two 16-byte pred stores
+// (pred and pmap are 256-byte aligned; n4 = n / 4, the tail done by thread 0).
+__device__ __forceinline__ void assemble_body(const int32_t* __restrict__ pmap, int64_t n,
+                                              const uint32_t* __restrict__ vis,
+                                              const int64_t* __restrict__ rp, int64_t root,
+                                              int64_t* __restrict__ pred) {
+  const int64_t n4 = n >> 2;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int4* m4 = reinterpret_cast<const int4*>(pmap);
+  longlong2* p2 = reinterpret_cast<longlong2*>(pred);
+  for (int64_t i = t0; i < n4; i += stride) {
+    const int4 m = __ldg(m4 + i);
+    const int64_t u = 4 * i;
+    p2[2 * i] = make_longlong2(assembled_entry(m.x, u, vis, rp, root),
+                               assembled_entry(m.y, u + 1, vis, rp, root));
+    p2[2 * i + 1] = make_longlong2(assembled_entry(m.z, u + 2, vis, rp, root),
+                                   assembled_entry(m.w, u + 3, vis, rp, root));
+  }
+  if (t0 == 0)
+    for (int64_t u = 4 * n4; u < n; ++u) pred[u] = assembled_entry(pmap[u], u, vis, rp, root);
+}
+
+__global__ void assemble_pred_kernel(const int32_t* __restrict__ pmap, int64_t n,
+                                     const uint32_t* __restrict__ vis,
+                                     const int64_t* __restrict__ rp, int64_t root,
+                                     int64_t* __restrict__ pred) {
+  assemble_body(pmap, n, vis, rp, root, pred);
+}
+
+// pmap from the row map and the CoreBFS tree parents (tp null without CoreBFS).
+__global__ void pred_map_kernel(const int32_t* __restrict__ rank, const int32_t* __restrict__ tp,
+                                int64_t nverts, int64_t n, int32_t* __restrict__ pmap) {
+  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    int32_t m = -1;
+    if (u < nverts) {
+      if (rank[u] >= 0) m = rank[u];
+      else if (tp && tp[u] >= 0) m = -tp[u] - 2;
+    }
+    pmap[u] = m;
+  }
+}
+
 // Edge-balanced top-down expansion.  Frontier queue[0..qsize) with
 // qdeg[i] = sum of degrees of queue[0..i) (qdeg[qsize] = total).
 // kWarpSearch: the tile's first row is found by a 32-way warp search
@@ -122,7 +194,8 @@ template <bool kWarpSearch, int kUnroll>
 __device__ __forceinline__ void td_expand_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
   const int64_t qsize = (int64_t)ctr->qsize;
   if (qsize == 0) return;
@@ -182,7 +255,7 @@ __device__ __forceinline__ void td_expand_body(
         if (us[j] < 0) continue;
         const uint32_t bit = 1u << (us[j] & 31);
         if ((words[j] & bit) == 0) {
-          pred[__ldg(inv + us[j])] = pred_entry(__ldg(inv + srcs[j]), level);
+          pred[pred_slot(pidx, us[j])] = pred_entry(__ldg(inv + srcs[j]), level);
           red_or(vis + (us[j] >> 5), bit);
         }
       }
@@ -198,6 +271,7 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
                                                  const int64_t* __restrict__ row_ptr,
                                                  const int32_t* __restrict__ col,
                                                  const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx,
                                                  int64_t* __restrict__ pred, int64_t level,
                                                  Counters* __restrict__ ctr) {
   const int lane = lane_id();
@@ -258,7 +332,7 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
       nxt[w] = c | fm;
       found_total += __popc(fm);
     }
-    if (parent >= 0) pred[__ldg(inv + v)] = pred_entry(__ldg(inv + parent), level);
+    if (parent >= 0) pred[pred_slot(pidx, v)] = pred_entry(__ldg(inv + parent), level);
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(kFull, scanned, o);
@@ -282,7 +356,8 @@ template <int kWords, bool kFirst>
 __device__ __forceinline__ void bu_wide_body(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ first, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ first, const int32_t* __restrict__ finv,
+    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
     int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -302,14 +377,22 @@ __device__ __forceinline__ void bu_wide_body(
     }
     int64_t b[kWords], e[kWords];
     int32_t par[kWords];
+    // original id of the parent when it is the first neighbour (from finv,
+    // loaded with first[]); -1: looked up in inv[] at the end
+    int32_t po[kWords];
     if (kFirst) {
-      int32_t f[kWords];
+      int32_t f[kWords], fo[kWords];
 #pragma unroll
       for (int k = 0; k < kWords; ++k) {
         par[k] = -1;
+        po[k] = -1;
         b[k] = e[k] = 0;
         f[k] = -1;
-        if (((~c[k]) >> lane) & 1u) f[k] = __ldg(first + (w0 + k) * 32 + lane);
+        fo[k] = -1;
+        if (((~c[k]) >> lane) & 1u) {
+          f[k] = __ldg(first + (w0 + k) * 32 + lane);
+          if (finv) fo[k] = __ldg(finv + (w0 + k) * 32 + lane);
+        }
       }
       uint32_t mf[kWords];
 #pragma unroll
@@ -320,6 +403,7 @@ __device__ __forceinline__ void bu_wide_body(
         scanned += 1;
         if ((mf[k] >> (f[k] & 31)) & 1u) {
           par[k] = f[k];
+          po[k] = fo[k];
         } else {
           const int64_t v = (w0 + k) * 32 + lane;
           b[k] = row_ptr[v] + 1;
@@ -330,6 +414,7 @@ __device__ __forceinline__ void bu_wide_body(
 #pragma unroll
       for (int k = 0; k < kWords; ++k) {
         par[k] = -1;
+        po[k] = -1;
         b[k] = e[k] = 0;
         if (((~c[k]) >> lane) & 1u) {
           const int64_t v = (w0 + k) * 32 + lane;
@@ -412,7 +497,7 @@ __device__ __forceinline__ void bu_wide_body(
       }
       if (par[k] >= 0) {
         const int64_t v = (w0 + k) * 32 + lane;
-        pred[__ldg(inv + v)] = pred_entry(__ldg(inv + par[k]), level);
+        pred[pred_slot(pidx, v)] = pred_entry(po[k] >= 0 ? po[k] : __ldg(inv + par[k]), level);
       }
     }
   }
@@ -431,7 +516,8 @@ __device__ __forceinline__ void bu_wide_body(
 __global__ void __launch_bounds__(256) td_wide_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
   const int64_t qsize = (int64_t)ctr->qsize;
   if (qsize == 0) return;
@@ -492,7 +578,7 @@ __global__ void __launch_bounds__(256) td_wide_kernel(
       if (us[k] < 0) continue;
       const uint32_t bit = 1u << (us[k] & 31);
       if ((words[k] & bit) == 0) {
-        pred[__ldg(inv + us[k])] = pred_entry(__ldg(inv + srcs[k]), level);
+        pred[pred_slot(pidx, us[k])] = pred_entry(__ldg(inv + srcs[k]), level);
         red_or(vis + (us[k] >> 5), bit);
       }
     }
@@ -511,7 +597,8 @@ __global__ void __launch_bounds__(256) td_wide_kernel(
 __device__ __forceinline__ void td_chunk_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
   __shared__ int s_map[8][32];
   const int64_t qsize = (int64_t)ctr->qsize;
@@ -563,7 +650,7 @@ __device__ __forceinline__ void td_chunk_body(
       const int32_t u = __ldg(col + rb + (e - lo));
       const uint32_t bit = 1u << (u & 31);
       if ((vis[u >> 5] & bit) == 0) {
-        pred[__ldg(inv + u)] = pred_entry(__ldg(inv + src), level);
+        pred[pred_slot(pidx, u)] = pred_entry(__ldg(inv + src), level);
         red_or(vis + (u >> 5), bit);
       }
     }
@@ -771,26 +858,30 @@ template <bool kWarpSearch, int kUnroll>
 __global__ void __launch_bounds__(256) td_expand_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
+  td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 template <int kWords, int kMinBlocks, bool kFirst>
 __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ first, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ first, const int32_t* __restrict__ finv,
+    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
     int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
-  bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, inv, pred, level, ctr);
+  bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred, level,
+                               ctr);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ inv, uint32_t* vis,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, level);
+  td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 template <bool kDeg>
@@ -850,11 +941,15 @@ __global__ void sg_root_kernel(const SgArg* __restrict__ a, const int32_t* __res
                                const int64_t* __restrict__ row_ptr, int64_t* __restrict__ pred,
                                uint32_t* __restrict__ vis0, uint32_t* __restrict__ vis1,
                                int32_t* __restrict__ queue, int64_t* __restrict__ qdeg,
-                               Counters* ctr, SingleCtl* __restrict__ c) {
+                               Counters* ctr, SingleCtl* __restrict__ c, int row_mode) {
   const int64_t root = a->root;
-  if (a->prev_root >= 0) pred[a->prev_root] = -1;
-  pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
   const int32_t r = rank[root];
+  if (row_mode) {  // as root_kernel
+    if (r >= 0) pred[r] = root;
+  } else {
+    if (a->prev_root >= 0) pred[a->prev_root] = -1;
+    pred[root] = root;  // level 0, first_expand (bfs.hpp:593)
+  }
   memset(ctr, 0, sizeof(Counters));
   if (r >= 0) {
     vis0[r >> 5] |= 1u << (r & 31);
@@ -893,6 +988,13 @@ __global__ void sg_reset_unvisited_kernel(const SingleCtl* __restrict__ c,
   }
 }
 
+__global__ void sg_assemble_kernel(const SingleCtl* __restrict__ c, const SgArg* __restrict__ a,
+                                   uint32_t* const* __restrict__ vis_pp,
+                                   const int32_t* __restrict__ pmap, int64_t n,
+                                   const int64_t* __restrict__ rp, int64_t* __restrict__ pred) {
+  assemble_body(pmap, n, vis_pp[c->cur], rp, a->root, pred);
+}
+
 // Level start (host loop: ++level, at[8], prev_nq, forward, clear counters).
 __global__ void sg_begin_kernel(SingleCtl* __restrict__ c, const SgArg* __restrict__ a,
                                 Counters* __restrict__ ctr) {
@@ -917,27 +1019,30 @@ __global__ void __launch_bounds__(256) sg_td_kernel(
     const SingleCtl* __restrict__ c, int td_form, const int32_t* __restrict__ queue,
     const int64_t* __restrict__ qdeg, const Counters* __restrict__ ctr,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ inv, uint32_t* const* __restrict__ vis_pp,
+    const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* const* __restrict__ vis_pp,
     int64_t* __restrict__ pred) {
   if (c->done || !c->forward) return;
   const int form = td_form == 4 ? (c->growing ? 5 : 3) : td_form;
   if (form != kForm) return;
   uint32_t* vis = vis_pp[c->cur];
   if (kForm == 3)
-    td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
+    td_chunk_body(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, c->level);
   else
-    td_expand_body<kForm == 5, 1>(queue, qdeg, ctr, row_ptr, col, inv, vis, pred, c->level);
+    td_expand_body<kForm == 5, 1>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, c->level);
 }
 
 template <bool kFirst>
 __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
     const SingleCtl* __restrict__ c, int64_t W, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ first,
-    const int32_t* __restrict__ inv, uint32_t* const* __restrict__ vis_pp,
+    const int32_t* __restrict__ finv, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* const* __restrict__ vis_pp,
     int64_t* __restrict__ pred, Counters* __restrict__ ctr) {
   if (c->done || c->forward) return;
   const int cur = c->cur;
-  bu_wide_body<4, kFirst>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, inv, pred,
+  bu_wide_body<4, kFirst>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, finv, inv, pidx,
+                          pred,
                           c->level, ctr);
 }
 
@@ -1073,6 +1178,23 @@ __global__ void sg_control_kernel(SingleCtl* __restrict__ c, const SgArg* __rest
 
 }  // namespace
 
+// Algorithmic bytes of the assembly pass: the map and pred over every id,
+// the rp entries of the reached rows, the visited bitmap.
+int64_t assembly_bytes(const BfsState& st, int64_t visited) {
+  return 12 * st.pred_size + 8 * visited + 4 * st.W;
+}
+
+void build_pred_assembly(DeviceArena& arena, const Graph& g, BfsState& st, cudaStream_t s,
+                         int sms) {
+  if (!st.rp) st.rp = arena_alloc<int64_t>(arena, st.R + 1, "row-order pred");
+  if (!st.pmap) st.pmap = arena_alloc<int32_t>(arena, st.pred_size + 4, "pred assembly map");
+  pred_map_kernel<<<grid_for(st.pred_size, 256, sms, 8), 256, 0, s>>>(
+      g.csr.rank, g.core.enabled ? g.core.tree_parent : nullptr, g.nverts, st.pred_size,
+      st.pmap);
+  check_cuda(cudaGetLastError(), "pred assembly map");
+  check_cuda(cudaStreamSynchronize(s), "pred assembly map");
+}
+
 void BfsState::allocate(DeviceArena& arena, const Graph& g) {
   release(arena);
   R = g.csr.nrows;
@@ -1094,6 +1216,7 @@ void BfsState::allocate(DeviceArena& arena, const Graph& g) {
   d_vis = arena_alloc<uint32_t*>(arena, 2, "bitmap pointers");
   pred_clean = false;
   prev_root = -1;
+  assembled = false;
   check_cuda(cudaMemcpy(d_vis, vis, sizeof(vis), cudaMemcpyHostToDevice), "bitmap pointers");
   check_cuda(cudaMallocHost(&hsctl, sizeof(SingleCtl)), "pinned control block");
   check_cuda(cudaMallocHost(&hsarg, sizeof(SgArg)), "pinned arguments");
@@ -1137,6 +1260,10 @@ void BfsState::release(DeviceArena& arena) {
   arena.free(blk_deg);
   arena.free(pred);
   arena.free(ctr);
+  if (rp) arena.free(rp);
+  if (pmap) arena.free(pmap);
+  rp = nullptr;
+  pmap = nullptr;
   cudaFreeHost(hctr);
   hctr = nullptr;
   allocated = false;
@@ -1155,24 +1282,23 @@ int chunk_blocks_per_sm() {
 
 // One level of the device-driven loop (captured into the WHILE body).
 void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
-                     int force_direction, bool bu_first, cudaGraphConditionalHandle cond) {
+                     int force_direction, bool bu_first, bool assemble,
+                     cudaGraphConditionalHandle cond) {
   const Csr& c = g.csr;
+  const int32_t* pidx = assemble ? nullptr : c.inv;
+  int64_t* out = assemble ? st.rp : st.pred;
   const int B = 256;
   const unsigned nblk = (unsigned)st.nblk;
   sg_begin_kernel<<<1, 1, 0, s>>>(st.sctl, st.sarg, st.ctr);
   sg_td_kernel<1><<<sms * 8, B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg, st.ctr, c.row_ptr,
-                                         c.col, c.inv, st.d_vis, st.pred);
+                                         c.col, c.inv, pidx, st.d_vis, out);
   sg_td_kernel<5><<<sms * 8, B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg, st.ctr, c.row_ptr,
-                                         c.col, c.inv, st.d_vis, st.pred);
+                                         c.col, c.inv, pidx, st.d_vis, out);
   sg_td_kernel<3><<<sms * chunk_blocks_per_sm(), B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg,
-                                                             st.ctr, c.row_ptr, c.col, c.inv,
-                                                             st.d_vis, st.pred);
-  if (bu_first && c.first)
-    sg_bu_kernel<true><<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.first, c.inv,
-                                             st.d_vis, st.pred, st.ctr);
-  else
-    sg_bu_kernel<false><<<sms * 4, B, 0, s>>>(st.sctl, st.W, c.row_ptr, c.col, c.first, c.inv,
-                                              st.d_vis, st.pred, st.ctr);
+                                                             st.ctr, c.row_ptr, c.col, c.inv, pidx,
+                                                             st.d_vis, out);
+  (bu_first && c.first ? sg_bu_kernel<true> : sg_bu_kernel<false>)<<<sms * 4, B, 0, s>>>(
+      st.sctl, st.W, c.row_ptr, c.col, c.first, c.first_inv, c.inv, pidx, st.d_vis, out, st.ctr);
   sg_count_kernel<false><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                          c.row_ptr, c.mdeg, st.blk_cnt,
                                                          st.blk_deg, st.ctr);
@@ -1189,19 +1315,21 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
 constexpr int kSgLevelLaunches = 12;
 
 std::vector<const void*> sg_key(const Graph& g, const BfsState& st, int sms, int td_form,
-                                int force_direction, bool bu_first) {
+                                int force_direction, bool bu_first, bool assemble) {
   const Csr& c = g.csr;
   return {st.sctl, st.sarg, st.d_vis, st.ctr, st.fr, st.queue, st.qdeg, st.blk_cnt, st.blk_deg,
           st.pred, st.vis[0], st.vis[1], c.row_ptr, c.col, c.inv, c.rank, c.mdeg,
           (const void*)(intptr_t)st.W, (const void*)(intptr_t)st.R,
           (const void*)(intptr_t)st.pred_size, (const void*)(intptr_t)c.nedges,
           (const void*)(intptr_t)sms, (const void*)(intptr_t)td_form,
-          (const void*)(intptr_t)force_direction, c.first, (const void*)(intptr_t)bu_first};
+          (const void*)(intptr_t)force_direction, c.first, c.first_inv,
+          (const void*)(intptr_t)bu_first,
+          (const void*)(intptr_t)assemble, st.rp, st.pmap};
 }
 
 // [init, root] then WHILE(level); the control kernel sets the condition.
 void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
-                    int force_direction, bool bu_first) {
+                    int force_direction, bool bu_first, bool assemble) {
   if (st.sgexec) cudaGraphExecDestroy(st.sgexec);
   if (st.sgraph) cudaGraphDestroy(st.sgraph);
   st.sgexec = nullptr;
@@ -1210,8 +1338,9 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
   check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
   init_kernel<<<grid_for(st.W, 256, sms, 8), 256, 0, s>>>(st.pred, st.pred_size, st.vis[0],
                                                           st.vis[1], st.W, st.R, 0);
-  sg_root_kernel<<<1, 1, 0, s>>>(st.sarg, c.rank, c.row_ptr, st.pred, st.vis[0], st.vis[1],
-                                 st.queue, st.qdeg, st.ctr, st.sctl);
+  sg_root_kernel<<<1, 1, 0, s>>>(st.sarg, c.rank, c.row_ptr, assemble ? st.rp : st.pred,
+                                 st.vis[0], st.vis[1], st.queue, st.qdeg, st.ctr, st.sctl,
+                                 assemble ? 1 : 0);
   cudaStreamCaptureStatus cs;
   const cudaGraphNode_t* deps = nullptr;
   size_t nd = 0;
@@ -1228,7 +1357,10 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
   if (err == cudaSuccess) err = cudaGraphAddNode(&node, cg, deps, nd, &p);
   if (err == cudaSuccess)
     err = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
-  if (err == cudaSuccess)
+  if (err == cudaSuccess && assemble)
+    sg_assemble_kernel<<<grid_for(st.pred_size / 4, 256, sms, 8), 256, 0, s>>>(
+        st.sctl, st.sarg, st.d_vis, st.pmap, st.pred_size, st.rp, st.pred);
+  else if (err == cudaSuccess)
     sg_reset_unvisited_kernel<<<grid_for(st.W, 256, sms, 8), 256, 0, s>>>(st.sctl, st.d_vis, st.W,
                                                                            c.inv, st.pred);
   cudaGraph_t body = err == cudaSuccess ? p.conditional.phGraph_out[0] : nullptr;
@@ -1240,7 +1372,7 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
     err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
-      sg_launch_level(g, st, s, sms, td_form, force_direction, bu_first, cond);
+      sg_launch_level(g, st, s, sms, td_form, force_direction, bu_first, assemble, cond);
       cudaGraph_t b2 = nullptr;
       err = cudaStreamEndCapture(s, &b2);
     }
@@ -1253,7 +1385,7 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
     cudaGetLastError();
     check_cuda(err, "search level-loop graph");
   }
-  st.skey = sg_key(g, st, sms, td_form, force_direction, bu_first);
+  st.skey = sg_key(g, st, sms, td_form, force_direction, bu_first, assemble);
 }
 
 // run_bfs_core with the level loop on the device.
@@ -1261,10 +1393,12 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
                         int64_t root_level, int edgefactor, double alpha, double beta,
                         int64_t* at, const RunOptions& opt, b200bfs_run_stats* stats) {
   const bool bu_first = opt.bu_first != 0;
+  const bool assemble = use_pred_assembly(g, opt);
+  if (assemble && !st.pmap) throw Error{B200BFS_ERR_STATE, "pred assembly map not built"};
   if (!st.sgexec ||
-      st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction, bu_first))
-    sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction, bu_first);
-  if (!st.pred_clean) {
+      st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction, bu_first, assemble))
+    sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction, bu_first, assemble);
+  if (!st.pred_clean && !assemble) {
     st.tree_clean = false;
     init_kernel<<<grid_for(st.pred_size / 2, 256, sms, 8), 256, 0, s>>>(
         st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, 1);
@@ -1289,6 +1423,7 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   if (c.done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
   st.pred_clean = true;
   st.prev_root = root;
+  st.assembled = assemble;
   if (at)
     for (int i = 0; i < 9; ++i) at[i] = c.at[i];
   st.levels.clear();
@@ -1308,7 +1443,9 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
     rs.edges_scanned_bu = c.scanned_bu;
     rs.td_bytes = c.td_bytes;
     rs.bu_bytes = c.bu_bytes;
-    rs.algorithmic_bytes = c.bytes + 4 * st.W + 8 * std::max<int64_t>(st.R - c.visited, 0);
+    rs.algorithmic_bytes =
+        c.bytes + 4 * st.W +
+        (assemble ? assembly_bytes(st, c.visited) : 8 * std::max<int64_t>(st.R - c.visited, 0));
     rs.kernel_launches = 3 + kSgLevelLaunches * (int)(c.num_td + c.num_bu);
     *stats = rs;
   }
@@ -1334,12 +1471,18 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   // (level kind, event index) of every timed level kernel
   std::vector<std::pair<bool, size_t>> timed;
   size_t nev = 0;
-  const bool fill_pred = !st.pred_clean;
+  // assemble: the levels write the row-order buffer rp and a final pass
+  // writes every pred entry; otherwise they write pred by original id
+  const bool assemble = use_pred_assembly(g, opt);
+  if (assemble && !st.pmap) throw Error{B200BFS_ERR_STATE, "pred assembly map not built"};
+  const int32_t* pidx = assemble ? nullptr : c.inv;
+  int64_t* out = assemble ? st.rp : st.pred;
+  const bool fill_pred = !st.pred_clean && !assemble;
   if (fill_pred) st.tree_clean = false;
   init_kernel<<<grid_for(std::max(fill_pred ? st.pred_size / 2 : 0, st.W), B, sms, 8), B, 0, s>>>(
       st.pred, st.pred_size, st.vis[0], st.vis[1], st.W, st.R, fill_pred ? 1 : 0);
-  root_kernel<<<1, 1, 0, s>>>(root, fill_pred ? -1 : st.prev_root, c.rank, c.row_ptr, st.pred,
-                              st.vis[0], st.vis[1], st.queue, st.qdeg, st.ctr);
+  root_kernel<<<1, 1, 0, s>>>(root, st.pred_clean ? st.prev_root : -1, c.rank, c.row_ptr, out,
+                              st.vis[0], st.vis[1], st.queue, st.qdeg, st.ctr, assemble ? 1 : 0);
   bytes += fill_pred ? 8 * st.pred_size : 4 * st.W;  // pred initialisation / unvisited reset
   int cur = 0;  // vis[cur] is the current visited bitmap
 
@@ -1372,24 +1515,23 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // chunked form once the search has come back from bottom-up (short
       // rows of the tail levels)
       const int td_form = opt.td_kernel == 4 ? (growing ? 5 : 3) : opt.td_kernel;
+      // every top-down form has the same parameters
+      auto launch_td = [&](auto kernel, int grid) {
+        kernel<<<grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv, pidx,
+                                  st.vis[cur], out, level);
+      };
       if (td_form == 5 && opt.td_unroll == 4)
-        td_expand_kernel<true, 4><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
-                                                        c.col, c.inv, st.vis[cur], st.pred, level);
+        launch_td(td_expand_kernel<true, 4>, td_grid);
       else if (td_form == 5 && opt.td_unroll == 2)
-        td_expand_kernel<true, 2><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
-                                                        c.col, c.inv, st.vis[cur], st.pred, level);
+        launch_td(td_expand_kernel<true, 2>, td_grid);
       else if (td_form == 5)
-        td_expand_kernel<true, 1><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr,
-                                                        c.col, c.inv, st.vis[cur], st.pred, level);
+        launch_td(td_expand_kernel<true, 1>, td_grid);
       else if (td_form == 1)
-        td_expand_kernel<false, 1><<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
-                                               st.vis[cur], st.pred, level);
+        launch_td(td_expand_kernel<false, 1>, td_grid);
       else if (td_form == 3)
-        td_chunk_kernel<<<td_chunk_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col,
-                                                    c.inv, st.vis[cur], st.pred, level);
+        launch_td(td_chunk_kernel, td_chunk_grid);
       else
-        td_wide_kernel<<<td_grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv,
-                                             st.vis[cur], st.pred, level);
+        launch_td(td_wide_kernel, td_grid);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 2;
       frontier_count_kernel<false><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
@@ -1400,39 +1542,27 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       ++rs.num_bu_levels;
       if (level < 64) rs.bu_level_mask |= 1ull << level;
       const bool first = opt.bu_first && c.first;
-      if (opt.bu_kernel == 2 && first)
-        bu_wide_kernel<2, 8, true><<<bu_wide_grid, B, 0, s>>>(
-            st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first, c.inv, st.pred, level,
-            st.ctr);
-      else if (opt.bu_kernel == 2)
-        bu_wide_kernel<2, 8, false><<<bu_wide_grid, B, 0, s>>>(
-            st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first, c.inv, st.pred, level,
-            st.ctr);
-      else if (opt.bu_kernel == 3 && first)
-        bu_wide_kernel<2, 6, true><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
-                                                         c.row_ptr, c.col, c.first, c.inv,
-                                                         st.pred, level, st.ctr);
+      auto launch_wide = [&](auto kernel, int grid) {
+        kernel<<<grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first,
+                                  c.first_inv, c.inv, pidx, out, level, st.ctr);
+      };
+      auto launch_bu = [&](auto kernel) {
+        kernel<<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.inv,
+                                     pidx, out, level, st.ctr);
+      };
+      if (opt.bu_kernel == 2)
+        launch_wide(first ? bu_wide_kernel<2, 8, true> : bu_wide_kernel<2, 8, false>,
+                    bu_wide_grid);
       else if (opt.bu_kernel == 3)
-        bu_wide_kernel<2, 6, false><<<sms * 6, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
-                                                          c.row_ptr, c.col, c.first, c.inv,
-                                                          st.pred, level, st.ctr);
-      else if (opt.bu_kernel == 4 && first)
-        bu_wide_kernel<4, 4, true><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
-                                                         c.row_ptr, c.col, c.first, c.inv,
-                                                         st.pred, level, st.ctr);
+        launch_wide(first ? bu_wide_kernel<2, 6, true> : bu_wide_kernel<2, 6, false>, sms * 6);
       else if (opt.bu_kernel == 4)
-        bu_wide_kernel<4, 4, false><<<sms * 4, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W,
-                                                          c.row_ptr, c.col, c.first, c.inv,
-                                                          st.pred, level, st.ctr);
+        launch_wide(first ? bu_wide_kernel<4, 4, true> : bu_wide_kernel<4, 4, false>, sms * 4);
       else if (opt.bu_probe <= 4)
-        bu_kernel<4><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
-                                           c.inv, st.pred, level, st.ctr);
+        launch_bu(bu_kernel<4>);
       else if (opt.bu_probe <= 8)
-        bu_kernel<8><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
-                                           c.inv, st.pred, level, st.ctr);
+        launch_bu(bu_kernel<8>);
       else
-        bu_kernel<16><<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
-                                            c.inv, st.pred, level, st.ctr);
+        launch_bu(bu_kernel<16>);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 1;
       cur ^= 1;
@@ -1512,12 +1642,23 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       qsize = global_nq_size;
     }
   }
-  reset_unvisited_kernel<<<grid_for(st.W, B, sms, 8), B, 0, s>>>(st.vis[cur], st.W, c.inv,
-                                                                 st.pred);
+  if (assemble) {
+    check_cuda(cudaEventRecord(st.event(nev), s), "event");
+    assemble_pred_kernel<<<grid_for(st.pred_size / 4, B, sms, 8), B, 0, s>>>(
+        st.pmap, st.pred_size, st.vis[cur], st.rp, root, st.pred);
+    check_cuda(cudaEventRecord(st.event(nev + 1), s), "event");
+    nev += 2;
+    rs.pred_bytes = assembly_bytes(st, visited);
+    bytes += rs.pred_bytes;
+  } else {
+    reset_unvisited_kernel<<<grid_for(st.W, B, sms, 8), B, 0, s>>>(st.vis[cur], st.W, c.inv,
+                                                                   st.pred);
+    bytes += 8 * std::max<int64_t>(st.R - visited, 0);
+  }
   ++launches;
-  bytes += 8 * std::max<int64_t>(st.R - visited, 0);
   st.pred_clean = true;
   st.prev_root = root;
+  st.assembled = assemble;
   check_cuda(cudaGetLastError(), "bfs");
   for (size_t k = 0; k < timed.size(); ++k) {
     const auto& t = timed[k];
@@ -1525,6 +1666,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     check_cuda(cudaEventElapsedTime(&ms, st.ev[t.second], st.ev[t.second + 1]), "elapsed");
     (t.first ? rs.td_ms : rs.bu_ms) += ms;
     if (k < st.levels.size()) st.levels[k].ms = ms;
+  }
+  if (assemble) {
+    float ms = 0;
+    check_cuda(cudaEventSynchronize(st.ev[nev - 1]), "assembly");
+    check_cuda(cudaEventElapsedTime(&ms, st.ev[nev - 2], st.ev[nev - 1]), "elapsed");
+    rs.pred_ms = ms;
   }
   rs.kernel_launches = launches;
   rs.levels = (int32_t)level;

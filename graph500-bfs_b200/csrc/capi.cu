@@ -400,9 +400,15 @@ int b200bfs_prepare(b200bfs_handle* h, int edgefactor, double alpha, double beta
     e.prepared = false;
     e.st.allocate(e.arena, e.g);
     try {
-      if (e.g.core.enabled)
+      if (e.g.core.enabled) {
+        // reads reachability from pred as the level kernels leave it
+        b200bfs::RunOptions direct = e.opt;
+        direct.pred_assemble = 0;
         b200bfs::core_reset_unreachable(e.arena, e.stream, e.sms, e.g, e.st, edgefactor, alpha,
-                                        beta, e.opt);
+                                        beta, direct);
+      }
+      if (b200bfs::use_pred_assembly(e.g, e.opt))
+        b200bfs::build_pred_assembly(e.arena, e.g, e.st, e.stream, e.sms);
     } catch (...) {
       cudaStreamSynchronize(e.stream);
       e.st.release(e.arena);
@@ -548,6 +554,11 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "force_direction") {
       require(value >= 0 && value <= 2, B200BFS_ERR_INVALID, "force_direction must be 0..2");
       e.opt.force_direction = (int)value;
+    } else if (n == "pred_assemble") {
+      require(value == 0 || value == 1, B200BFS_ERR_INVALID, "pred_assemble must be 0 or 1");
+      e.opt.pred_assemble = (int)value;
+      if (e.prepared && !e.st.pmap && b200bfs::use_pred_assembly(e.g, e.opt))
+        b200bfs::build_pred_assembly(e.arena, e.g, e.st, e.stream, e.sms);
     } else {
       throw b200bfs::Error{B200BFS_ERR_INVALID, "unknown option " + n};
     }

@@ -19,6 +19,14 @@ __host__ __device__ __forceinline__ int64_t pred_entry(int64_t parent, int64_t l
                    ((uint64_t)parent & 0xFFFFFFFFFFFFull));
 }
 
+// Slot of row v's entry in the buffer a search kernel writes: the row's
+// original id (pidx = row -> original id map, the pred array itself), or v
+// when pidx is null and the kernel writes the row-order buffer that the
+// assembly pass turns into pred.
+__device__ __forceinline__ int64_t pred_slot(const int32_t* __restrict__ pidx, int64_t v) {
+  return pidx ? (int64_t)__ldg(pidx + v) : v;
+}
+
 __device__ __forceinline__ bool bit_test(const uint32_t* bm, int64_t v) {
   return (__ldg(bm + (v >> 5)) >> (v & 31)) & 1u;
 }

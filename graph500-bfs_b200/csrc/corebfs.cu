@@ -382,6 +382,7 @@ void build_core(DeviceArena& arena, cudaStream_t s, Graph& g, int sms) {
   arena.free(c.rank);
   arena.free(c.mdeg);
   arena.free(c.first);
+  arena.free(c.first_inv);
   c = k2;
   build_first(arena, s, c, sms);
   k.enabled = true;
@@ -489,7 +490,21 @@ void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   run_bfs_core(g, st, s, sms, u, lv, edgefactor, alpha, beta, at, opt, stats);
   int launches;
   int64_t bytes;
-  if (!st.tree_clean) {
+  if (st.assembled) {
+    // the assembly pass wrote every tree parent with level 0xFFFF: only this
+    // climb differs
+    RewriteArg a;
+    a.n = (int)pv.size();
+    for (size_t i = 0; i < pv.size(); ++i) {
+      a.v[i] = pv[i];
+      a.e[i] = pe[i];
+    }
+    rewrite_kernel<<<1, 128, 0, s>>>(a, st.pred);
+    check_cuda(cudaGetLastError(), "core climb");
+    launches = 1;
+    bytes = 16 * a.n;
+    st.tree_clean = true;
+  } else if (!st.tree_clean) {
     // write_tree_parents (corebfs_adaptor.hpp:285-301): every pruned vertex
     launches = core_write_tree(g, st.pred, pv, pe, s, sms);
     bytes = 16 * g.core.tree_vertices;

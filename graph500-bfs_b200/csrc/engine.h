@@ -91,6 +91,10 @@ struct Csr {
   // reference keeps each row's first edge apart too: isolated_edges_,
   // graph_constructor.hpp:1224-1348)
   int32_t* first = nullptr;
+  // [R] original id of the first neighbour (inv[first[r]]), read beside
+  // first[] so that a bottom-up parent found by the first probe needs no
+  // random gather into inv[] for the pred entry (null in the batch view)
+  int32_t* first_inv = nullptr;
   int64_t max_degree = 0;
 };
 
@@ -125,8 +129,8 @@ struct Graph {
   int64_t device_bytes = 0;
 };
 
-// Fills c.first from c.row_ptr and c.col.
-void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms);
+// Fills c.first from c.row_ptr and c.col, and c.first_inv when parent_ids.
+void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms, bool parent_ids = true);
 
 // Builds g.csr from nedges device edges (each a (v0, v1) pair of uint32 ids).
 void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t nedges,

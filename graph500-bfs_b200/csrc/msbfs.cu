@@ -774,7 +774,7 @@ void ensure_batch_view(DeviceArena& arena, Graph& g, cudaStream_t s, int sms) {
   v.col = arena_alloc<int32_t>(arena, c.nedges, "view adjacency");
   bview_copy_kernel<<<grid_for(R * 32, B, sms, 8), B, 0, s>>>(order, R, c.row_ptr, c.col,
                                                                g.b_of_row, v.row_ptr, v.col);
-  build_first(arena, s, v, sms);
+  build_first(arena, s, v, sms, false);
   check_cuda(cudaStreamSynchronize(s), "batch view");
   arena.free(order);
   g.bview = v;
@@ -1152,6 +1152,7 @@ void batch_select(const Graph& g, BfsState& st, const BatchState& bs, cudaStream
   // pred now holds exactly this root's result; its entry vertex is the one
   // entry outside the rows of the searched graph that a later search resets
   st.pred_clean = true;
+  st.assembled = false;
   st.prev_root = bs.entry_vertex[(size_t)index];
   if (g.core.enabled) {
     st.tree_clean = true;  // core_write_tree wrote every tree parent

@@ -102,6 +102,8 @@ typedef struct b200bfs_run_stats {
   double device_ms;              /* CUDA-event time of the whole run         */
   double td_ms;                  /* CUDA-event time of the top-down kernels  */
   double bu_ms;                  /* CUDA-event time of the bottom-up kernels */
+  int64_t pred_bytes;            /* bytes of the pred assembly pass (0: none) */
+  double pred_ms;                /* CUDA-event time of the pred assembly pass */
 } b200bfs_run_stats;
 
 /* One level of the last search (the per-level report of the reference's
@@ -270,9 +272,15 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
 
 /* Engine tuning knobs (no counterpart in the reference, whose equivalents
  * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
- * kernel form), "td_kernel" (1..5, top-down kernel form; 4 picks per level), "bu_probe" (1..64,
- * neighbours probed per lane by bottom-up form 1), "force_direction" (0 =
- * alpha/beta rule, 1 = top-down only, 2 = bottom-up from level 2),
+ * kernel form), "td_kernel" (1..5, top-down kernel form; 4 picks per
+ * level), "bu_probe" (1..64, neighbours probed per lane by bottom-up form
+ * 1), "bu_first" (1: bottom-up forms 2-4 probe the first neighbour from a
+ * dense per-row array first, the default), "td_unroll" (1, 2 or 4: 32-entry
+ * steps a lane of top-down form 5 handles together), "pred_assemble" (1:
+ * the levels write a row-order buffer and one pass over the original ids
+ * writes pred, the default; 0: the levels write pred by original id),
+ * "force_direction" (0 = alpha/beta rule, 1 = top-down only, 2 = bottom-up
+ * from level 2),
  * "single_graph" (1: b200bfs_run runs its level loop as a CUDA graph on the
  * device, one host synchronisation per search, with bottom-up form 4 and
  * top-down forms 1, 3, 4 or 5; per-level kernel times are then not

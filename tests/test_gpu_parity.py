@@ -176,14 +176,17 @@ def test_group_reorder(engine, oracle_graphs):
     engine.end()
 
 
-@pytest.mark.parametrize("scale", [12, 16, 18])
-def test_corebfs_parity(engine, oracle_graphs, scale):
+@pytest.mark.parametrize("scale,assemble", [(12, 0), (16, 0), (18, 0), (12, 1), (16, 1)])
+def test_corebfs_parity(engine, oracle_graphs, scale, assemble):
+    """assemble 1: tree parents come from the assembly pass's map, the climb
+    is written after it."""
     import b200bfs
 
     edges, g = oracle_graphs(scale)
     core = O.Core(g)
     engine.generate_graph(scale, 16, flags=b200bfs.BUILD_COREBFS)
     engine.prepare(16)
+    engine.set_option("pred_assemble", assemble)
     gi = engine.info()
     assert gi.corebfs == 1 and gi.prune_rounds == core.rounds
     assert gi.num_global_verts == core.core_num_verts
@@ -220,6 +223,7 @@ def test_corebfs_parity(engine, oracle_graphs, scale):
         tree = O.pred_levels(ref_pred) == 0xFFFF
         assert np.array_equal(pred[tree], ref_pred[tree])
         assert np.array_equal(O.pred_levels(pred), O.pred_levels(ref_pred))
+    engine.set_option("pred_assemble", 1)
     engine.end()
 
 
@@ -346,13 +350,15 @@ def test_device_level_loop_matches_host_loop(engine, oracle_graphs, alpha, beta,
         engine.end()
 
 
-@pytest.mark.parametrize("single_graph", [0, 1])
-def test_pred_exact_across_searches(engine, oracle_graphs, single_graph):
-    """pred is not refilled with -1 before every search: each search resets
-    the rows it leaves unreached and the previous root's entry.  Searches
-    that reach different vertex sets (giant component, a small component, an
-    isolated vertex, a batch result in between) must each leave exactly
-    their own result."""
+@pytest.mark.parametrize("single_graph,assemble", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_pred_exact_across_searches(engine, oracle_graphs, single_graph, assemble):
+    """Without the assembly pass pred is not refilled with -1 before every
+    search: each search resets the rows it leaves unreached and the previous
+    root's entry.  With it (pred_assemble 1) every entry is rewritten from the
+    row-order buffer, whose rows a search did not reach hold stale entries.
+    Searches that reach different vertex sets (giant component, a small
+    component, an isolated vertex, a batch result in between, a switch of
+    the option) must each leave exactly their own result."""
     edges, g = oracle_graphs(16)
     engine.generate_graph(16, 16)
     engine.prepare(16)
@@ -366,21 +372,29 @@ def test_pred_exact_across_searches(engine, oracle_graphs, single_graph):
             break
     assert small is not None
     isolated = int(np.nonzero(he == 0)[0][0])
+    def check(r):
+        engine.run(r)
+        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r)), r
+        pred = engine.get_pred()
+        assert np.all(pred[g.nverts:] == -1)
+        assert np.all(pred[: g.nverts][g.levels(r) < 0] == -1), r
+        err, _ = engine.validate(r)
+        assert err == 0, r
+
     try:
         engine.set_option("single_graph", single_graph)
+        engine.set_option("pred_assemble", assemble)
         for r in [big[0], small, big[1], isolated, small, big[0]]:
-            engine.run(r)
-            assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r)), r
-            assert np.all(engine.get_pred()[g.nverts:] == -1)
-            err, _ = engine.validate(r)
-            assert err == 0, r
+            check(r)
         engine.run_batch([small, big[1]])
         engine.batch_select(0)
-        engine.run(big[0])
-        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(big[0]))
+        check(big[0])
         engine.batch_select(1)
-        engine.run(small)
-        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(small))
+        check(small)
+        engine.set_option("pred_assemble", 1 - assemble)
+        for r in [big[1], small, isolated]:
+            check(r)
     finally:
         engine.set_option("single_graph", 0)
+        engine.set_option("pred_assemble", 1)
         engine.end()
