@@ -554,6 +554,14 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "force_direction") {
       require(value >= 0 && value <= 2, B200BFS_ERR_INVALID, "force_direction must be 0..2");
       e.opt.force_direction = (int)value;
+    } else if (n == "batch_probe") {
+      require(value == 4 || value == 8 || value == 16 || value == 32 || value == 64 ||
+                  value == 128 || value == 256 || value == 1024,
+              B200BFS_ERR_INVALID, "batch_probe must be 4, 8, 16, 32, 64, 128, 256 or 1024");
+      e.bs.bu_probe = (int)value;
+    } else if (n == "batch_round") {
+      require(value == 4 || value == 8, B200BFS_ERR_INVALID, "batch_round must be 4 or 8");
+      e.bs.bu_round = (int)value;
     } else if (n == "pred_assemble") {
       require(value == 0 || value == 1, B200BFS_ERR_INVALID, "pred_assemble must be 0 or 1");
       e.opt.pred_assemble = (int)value;

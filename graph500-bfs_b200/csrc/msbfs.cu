@@ -299,9 +299,11 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // Bottom-up pull for the roots in bu_mask_active.  A warp owns 32
 // consecutive rows (one per lane).  A lane whose row misses some of those
 // roots (U = ~seen & mask) ORs the frontier masks planes[L-1][u] of its
-// neighbours, kProbe of them four loads at a time, until every bit of U is
-// found; rows still open after that are swept by the whole warp, 32
-// neighbours per step, stopping as soon as U is covered.  Rows are sorted by
+// neighbours, up to kProbe of them kPer loads at a time, until every bit of
+// U is found; rows still open after that (long lists) are swept by the whole
+// warp, 32 neighbours per step, stopping as soon as U is covered.  The warp
+// sweep serves one row at a time, so most rows are best finished by their
+// own lane (kProbe 128 measured fastest).  Rows are sorted by
 // descending degree, so neighbour lists start with the hubs, which most
 // roots reach first.  The row's new bits are written to planes[L] and seen
 // by the lane that owns it, and every row of planes[L] is written (zero when
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // first (may be null): the rows' first neighbours; an open row ORs its first
 // neighbour's mask (one coalesced read of first[] per warp) before loading
 // its row offsets, which it then needs only if that mask does not cover U.
-template <int kProbe>
+template <int kProbe, int kPer>
 __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ctl,
                                                        const int64_t* __restrict__ row_ptr,
                                                        const int32_t* __restrict__ col,
@@ -357,17 +359,21 @@ __global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ct
       e = row_ptr[v + 1];
     }
 #pragma unroll 1
-    for (int p = 0; p < kProbe; p += 4) {
+    for (int p = 0; p < kProbe; p += kPer) {
       const bool need = (acc & U) != U && j < e;
       if (!__any_sync(kFull, need)) break;
       if (need) {
+        // kPer neighbour ids, then their masks (entries beyond the row
+        // repeat the first)
         const int64_t r = e - j;
-        const int32_t u0 = __ldg(col + j);
-        const int32_t u1 = r > 1 ? __ldg(col + j + 1) : u0;
-        const int32_t u2 = r > 2 ? __ldg(col + j + 2) : u0;
-        const int32_t u3 = r > 3 ? __ldg(col + j + 3) : u0;
-        acc |= __ldg(prev + u0) | __ldg(prev + u1) | __ldg(prev + u2) | __ldg(prev + u3);
-        const int64_t t = r < 4 ? r : 4;
+        int32_t u[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) u[q] = (q == 0 || r > q) ? __ldg(col + j + q) : u[0];
+        unsigned long long m = 0;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) m |= __ldg(prev + u[q]);
+        acc |= m;
+        const int64_t t = r < kPer ? r : kPer;
         j += t;
         scanned += t;
       }
@@ -905,7 +911,23 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
   batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
                                                       bs.queue, bs.qdeg);
   if (ev) check_cuda(cudaEventRecord(ev[1], s), "event");
-  batch_bu_kernel<8><<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
+  auto bu = batch_bu_kernel<128, 4>;
+  switch (bs.bu_probe * 16 + bs.bu_round) {
+    case 4 * 16 + 4: bu = batch_bu_kernel<4, 4>; break;
+    case 8 * 16 + 4: bu = batch_bu_kernel<8, 4>; break;
+    case 16 * 16 + 4: bu = batch_bu_kernel<16, 4>; break;
+    case 32 * 16 + 4: bu = batch_bu_kernel<32, 4>; break;
+    case 64 * 16 + 4: bu = batch_bu_kernel<64, 4>; break;
+    case 256 * 16 + 4: bu = batch_bu_kernel<256, 4>; break;
+    case 1024 * 16 + 4: bu = batch_bu_kernel<1024, 4>; break;
+    case 8 * 16 + 8: bu = batch_bu_kernel<8, 8>; break;
+    case 16 * 16 + 8: bu = batch_bu_kernel<16, 8>; break;
+    case 32 * 16 + 8: bu = batch_bu_kernel<32, 8>; break;
+    case 64 * 16 + 8: bu = batch_bu_kernel<64, 8>; break;
+    case 128 * 16 + 8: bu = batch_bu_kernel<128, 8>; break;
+    default: break;
+  }
+  bu<<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
   batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg, c.row_ptr, c.col);
   if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
@@ -925,7 +947,8 @@ std::vector<const void*> graph_key_of(const Graph& g, const BatchState& bs, int 
   const Csr& c = batch_csr(g);
   return {bs.ctl, bs.d_arg, bs.blk_cnt, bs.blk_deg, (const void*)(intptr_t)bs.nblk,
           (const void*)(intptr_t)bs.R, c.row_ptr, c.col, c.mdeg, c.first, g.csr.rank, g.b_of_row,
-          (const void*)(intptr_t)g.nverts, bs.queue, bs.qdeg, (const void*)(intptr_t)sms};
+          (const void*)(intptr_t)g.nverts, bs.queue, bs.qdeg, (const void*)(intptr_t)sms,
+          (const void*)(intptr_t)bs.bu_probe, (const void*)(intptr_t)bs.bu_round};
 }
 
 // Prologue (zero, setup, first control) followed by a WHILE node whose body

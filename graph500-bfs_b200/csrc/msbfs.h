@@ -87,6 +87,11 @@ struct BatchState {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<const void*> graph_key;
   // last batch
+  // neighbours a lane probes in the bottom-up sweep before the warp sweeps
+  // its row (4 .. 1024), bu_round of them loaded together (4 or 8).  SCALE 28,
+  // 64 roots: 8 / 32 / 128 / 1024 probes give 29.0 / 26.2 / 24.3 / 24.6 ms.
+  int bu_probe = 128;
+  int bu_round = 4;
   int K = 0;
   int64_t levels = 0;                 // planes in use = last level + 1
   std::vector<int64_t> roots;         // original ids
