@@ -1271,14 +1271,6 @@ void BfsState::release(DeviceArena& arena) {
 
 namespace {
 
-int chunk_blocks_per_sm() {
-  static int per_sm = 0;
-  if (!per_sm &&
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_chunk_kernel, 256, 0) !=
-          cudaSuccess)
-    per_sm = 4;
-  return std::max(per_sm, 1);
-}
 
 // One level of the device-driven loop (captured into the WHILE body).
 void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int td_form,
@@ -1294,7 +1286,8 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
                                          c.col, c.inv, pidx, st.d_vis, out);
   sg_td_kernel<5><<<sms * 8, B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg, st.ctr, c.row_ptr,
                                          c.col, c.inv, pidx, st.d_vis, out);
-  sg_td_kernel<3><<<sms * chunk_blocks_per_sm(), B, 0, s>>>(st.sctl, td_form, st.queue, st.qdeg,
+  sg_td_kernel<3><<<sms * blocks_per_sm(td_chunk_kernel, 256), B, 0, s>>>(st.sctl, td_form,
+                                                                          st.queue, st.qdeg,
                                                              st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                                              st.d_vis, out);
   (bu_first && c.first ? sg_bu_kernel<true> : sg_bu_kernel<false>)<<<sms * 4, B, 0, s>>>(
@@ -1335,6 +1328,7 @@ void sg_build_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, int t
   st.sgexec = nullptr;
   st.sgraph = nullptr;
   const Csr& c = g.csr;
+  blocks_per_sm(td_chunk_kernel, 256);  // occupancy queries stay outside the capture
   check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
   init_kernel<<<grid_for(st.W, 256, sms, 8), 256, 0, s>>>(st.pred, st.pred_size, st.vis[0],
                                                           st.vis[1], st.W, st.R, 0);
@@ -1491,12 +1485,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   int64_t global_nq_size = 0, global_nq_edges = 0;
   int64_t visited = 1, qsize = 1;
   st.levels.clear();
-  const int td_grid = sms * 8;
-  const int bu_grid = grid_for(st.W * 32, B, sms, 8);
+  const int bu_grid =
+      std::min(grid_for(st.W * 32, B, sms, 8), sms * blocks_per_sm(bu_kernel<8>, B));
   const int bu_wide_grid = sms * 8;
   // the chunked top-down form splits the work evenly over its warps, so its
   // grid is exactly the resident blocks (one wave)
-  const int td_chunk_grid = sms * chunk_blocks_per_sm();
+  const int td_chunk_grid = sms * blocks_per_sm(td_chunk_kernel, 256);
   for (;;) {
     ++level;
     if (level > kMaxLevel) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
@@ -1516,22 +1510,24 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // rows of the tail levels)
       const int td_form = opt.td_kernel == 4 ? (growing ? 5 : 3) : opt.td_kernel;
       // every top-down form has the same parameters
+      // one resident wave of each form (their register counts differ)
       auto launch_td = [&](auto kernel, int grid) {
+        if (grid <= 0) grid = sms * blocks_per_sm(kernel, B);
         kernel<<<grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                   st.vis[cur], out, level);
       };
       if (td_form == 5 && opt.td_unroll == 4)
-        launch_td(td_expand_kernel<true, 4>, td_grid);
+        launch_td(td_expand_kernel<true, 4>, 0);
       else if (td_form == 5 && opt.td_unroll == 2)
-        launch_td(td_expand_kernel<true, 2>, td_grid);
+        launch_td(td_expand_kernel<true, 2>, 0);
       else if (td_form == 5)
-        launch_td(td_expand_kernel<true, 1>, td_grid);
+        launch_td(td_expand_kernel<true, 1>, 0);
       else if (td_form == 1)
-        launch_td(td_expand_kernel<false, 1>, td_grid);
+        launch_td(td_expand_kernel<false, 1>, 0);
       else if (td_form == 3)
         launch_td(td_chunk_kernel, td_chunk_grid);
       else
-        launch_td(td_wide_kernel, td_grid);
+        launch_td(td_wide_kernel, 0);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 2;
       frontier_count_kernel<false><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(

@@ -3,6 +3,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <cuda_runtime.h>
 
 namespace b200bfs {
@@ -17,6 +19,29 @@ constexpr int64_t kMaxLevel = 0xFFFE;
 __host__ __device__ __forceinline__ int64_t pred_entry(int64_t parent, int64_t level) {
   return (int64_t)(((uint64_t)(level & 0xFFFF) << 48) |
                    ((uint64_t)parent & 0xFFFFFFFFFFFFull));
+}
+
+// Blocks of `block` threads of `kernel` resident on one SM (at least 1),
+// cached per kernel.  Grid-stride kernels launched with exactly
+// blocks_per_sm * SMs blocks run in one wave: a grid larger than what is
+// resident leaves the blocks that do not fit for a second, mostly idle
+// wave.
+template <typename K>
+int blocks_per_sm(K kernel, int block) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), block);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess ||
+      n < 1) {
+    cudaGetLastError();
+    n = 1;
+  }
+  cache[key] = n;
+  return n;
 }
 
 // Slot of row v's entry in the buffer a search kernel writes: the row's

@@ -314,8 +314,9 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // first (may be null): the rows' first neighbours; an open row ORs its first
 // neighbour's mask (one coalesced read of first[] per warp) before loading
 // its row offsets, which it then needs only if that mask does not cover U.
+// Launched with 4 blocks per SM, all resident (at most 64 registers).
 template <int kProbe, int kPer>
-__global__ void __launch_bounds__(256) batch_bu_kernel(BatchCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(256, 4) batch_bu_kernel(BatchCtl* __restrict__ ctl,
                                                        const int64_t* __restrict__ row_ptr,
                                                        const int32_t* __restrict__ col,
                                                        const int32_t* __restrict__ first) {
@@ -440,6 +441,8 @@ __global__ void __launch_bounds__(256) batch_stats_kernel(BatchCtl* __restrict__
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  // lane j accumulates roots j and j + 32 in registers
+  unsigned long long c_lo = 0, c_hi = 0, e_lo = 0, e_hi = 0;
   for (int64_t w = gw; w < head_w + tail_w; w += nwarps) {
     int64_t v;
     unsigned long long wt;
@@ -460,11 +463,24 @@ __global__ void __launch_bounds__(256) batch_stats_kernel(BatchCtl* __restrict__
       const bool b = (n >> k) & 1ull;
       const unsigned c = __popc(__ballot_sync(kFull, b));
       const unsigned ds = __reduce_add_sync(kFull, b ? d : 0u);
-      if (lane == 0) {
-        atomicAdd(&s_cnt[k], (unsigned long long)c * wt);
-        atomicAdd(&s_edg[k], (unsigned long long)ds * wt);
+      if (lane == (k & 31)) {
+        if (k < 32) {
+          c_lo += (unsigned long long)c * wt;
+          e_lo += (unsigned long long)ds * wt;
+        } else {
+          c_hi += (unsigned long long)c * wt;
+          e_hi += (unsigned long long)ds * wt;
+        }
       }
     }
+  }
+  if (c_lo) {
+    atomicAdd(&s_cnt[lane], c_lo);
+    atomicAdd(&s_edg[lane], e_lo);
+  }
+  if (c_hi) {
+    atomicAdd(&s_cnt[lane + 32], c_hi);
+    atomicAdd(&s_edg[lane + 32], e_hi);
   }
   __syncthreads();
   if (threadIdx.x < kBatchMax && s_cnt[threadIdx.x]) {
@@ -486,78 +502,96 @@ __global__ void __launch_bounds__(256) batch_stats_kernel(BatchCtl* __restrict__
 //  - done = 1 when no root has a frontier and none is still to enter,
 //    2 when planes[L + 1] is not allocated, 3 past level 0xFFFE.
 // With a graph conditional handle it also sets the loop condition.
-__global__ void batch_control_kernel(BatchCtl* __restrict__ ctl, const int32_t* __restrict__ mdeg,
-                                     cudaGraphConditionalHandle cond, int use_cond) {
+// One thread per root (kBatchMax threads): each seeds and tests its own
+// root; the mask updates are gathered in shared memory and thread 0 plans
+// the next level.
+__global__ void __launch_bounds__(kBatchMax) batch_control_kernel(
+    BatchCtl* __restrict__ ctl, const int32_t* __restrict__ mdeg,
+    cudaGraphConditionalHandle cond, int use_cond) {
+  __shared__ unsigned long long s_seeded, s_entered, s_bu_set, s_bu_clr, s_grow_clr;
   BatchCtl& c = *ctl;
+  const int k = threadIdx.x;
+  const unsigned long long bit = 1ull << k;
   const long long L = c.level;
-  unsigned long long* cur = plane_ptr(ctl, L);
-  unsigned long long seeded = 0;
-  unsigned long long pend = c.pending;
-  while (pend) {
-    const int k = __ffsll((long long)pend) - 1;
-    pend &= pend - 1;
-    if (c.root_lv[k] != L) continue;
-    const unsigned long long bit = 1ull << k;
-    c.pending &= ~bit;
+  if (k == 0) s_seeded = s_entered = s_bu_set = s_bu_clr = s_grow_clr = 0;
+  __syncthreads();
+  const unsigned long long pending = c.pending;
+  if ((pending & bit) && c.root_lv[k] == L) {
+    atomicOr(&s_entered, bit);
     const int r = c.root_row[k];
-    if (r < 0) continue;
-    cur[r] |= bit;
-    c.seen[r] |= bit;
-    c.rowbits[L & 1][r >> 5] |= 1u << (r & 31);
-    c.c.active |= bit;
-    seeded |= bit;
+    if (r >= 0) {
+      atomicOr(plane_ptr(ctl, L) + r, bit);
+      atomicOr(c.seen + r, bit);
+      atomicOr(c.rowbits[L & 1] + (r >> 5), 1u << (r & 31));
+      atomicOr(&s_seeded, bit);
+    }
   }
-  if (L < kBatchHist) {
-    BatchLevelRec& h = c.hist[L];
-    h.td_roots = c.has_td ? c.td_mask : 0ull;
-    h.bu_roots = c.has_bu ? c.bu_mask_active : 0ull;
-    h.active = c.c.active;
-    h.scanned_bu = c.c.scanned_bu;
-    h.rows_bu = c.c.rows_bu;
-    h.qsize = c.has_td ? c.c.qsize : 0ull;
-    h.qedges = c.has_td ? c.c.qedges : 0ull;
-  }
-  const unsigned long long act = c.c.active;
-  const long long e_thr = (long long)(c.nedges / c.alpha);
-  const long long n_thr = (long long)(c.nverts / (c.beta * c.edgefactor * 2.0));
-  unsigned long long it = act & ~seeded;
-  while (it) {
-    const int k = __ffsll((long long)it) - 1;
-    it &= it - 1;
-    const unsigned long long bit = 1ull << k;
+  __syncthreads();
+  const unsigned long long seeded = s_seeded;
+  const unsigned long long act = c.c.active | seeded;
+  if ((act & ~seeded) & bit) {
+    const long long e_thr = (long long)(c.nedges / c.alpha);
+    const long long n_thr = (long long)(c.nverts / (c.beta * c.edgefactor * 2.0));
     const long long n = (long long)c.c.cnt[k], e = (long long)c.c.edg[k];
+    const unsigned long long bu = c.bu_mask;
     if ((c.growing & bit) && n > c.prev_cnt[k]) {
-      if (!(c.bu_mask & bit) && e > e_thr) c.bu_mask |= bit;
-    } else if (c.bu_mask & bit) {
+      if (!(bu & bit) && e > e_thr) atomicOr(&s_bu_set, bit);
+    } else if (bu & bit) {
       if (n < n_thr) {
-        c.bu_mask &= ~bit;
-        c.growing &= ~bit;
+        atomicOr(&s_bu_clr, bit);
+        atomicOr(&s_grow_clr, bit);
       }
     }
     c.prev_cnt[k] = n;
   }
-  unsigned long long sd = seeded;
-  while (sd) {
-    const int k = __ffsll((long long)sd) - 1;
-    sd &= sd - 1;
-    c.prev_cnt[k] = 0;
+  if (seeded & bit) c.prev_cnt[k] = 0;
+  __syncthreads();
+  if (k == 0) {
+    c.pending = pending & ~s_entered;
+    c.c.active = act;
+    if (L < kBatchHist) {
+      BatchLevelRec& h = c.hist[L];
+      h.td_roots = c.has_td ? c.td_mask : 0ull;
+      h.bu_roots = c.has_bu ? c.bu_mask_active : 0ull;
+      h.active = act;
+      h.scanned_bu = c.c.scanned_bu;
+      h.rows_bu = c.c.rows_bu;
+      h.qsize = c.has_td ? c.c.qsize : 0ull;
+      h.qedges = c.has_td ? c.c.qedges : 0ull;
+    }
+    const unsigned long long bu_mask = (c.bu_mask | s_bu_set) & ~s_bu_clr;
+    c.bu_mask = bu_mask;
+    c.growing &= ~s_grow_clr;
+    int done = 0;
+    if (act == 0 && c.pending == 0) {
+      done = 1;
+    } else if (L + 1 > kMaxLevel) {
+      done = 3;
+    } else {
+      c.level = L + 1;
+      c.td_mask = act & ~bu_mask;
+      c.bu_mask_active = act & bu_mask;
+      c.has_td = c.td_mask != 0;
+      c.has_bu = c.bu_mask_active != 0;
+      if (L + 1 >= c.capacity) done = 2;
+    }
+    c.done = done;
+    if (use_cond) cudaGraphSetConditional(cond, done == 0 ? 1u : 0u);
   }
-  int done = 0;
-  if (act == 0 && c.pending == 0) {
-    done = 1;
-  } else if (L + 1 > kMaxLevel) {
-    done = 3;
-  } else {
-    c.level = L + 1;
-    c.td_mask = act & ~c.bu_mask;
-    c.bu_mask_active = act & c.bu_mask;
-    c.has_td = c.td_mask != 0;
-    c.has_bu = c.bu_mask_active != 0;
-    memset(&c.c, 0, sizeof(BatchCounters));
-    if (L + 1 >= c.capacity) done = 2;
+  __syncthreads();
+  // the next level's counters start at zero (not when the search stops:
+  // the host reads them)
+  if (c.done == 0 || c.done == 2) {
+    c.c.cnt[k] = 0;
+    c.c.edg[k] = 0;
+    if (k == 0) {
+      c.c.active = 0;
+      c.c.scanned_bu = 0;
+      c.c.rows_bu = 0;
+      c.c.qsize = 0;
+      c.c.qedges = 0;
+    }
   }
-  c.done = done;
-  if (use_cond) cudaGraphSetConditional(cond, done == 0 ? 1u : 0u);
 }
 
 struct BatchSetupArg {
@@ -929,10 +963,11 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
   }
   bu<<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
-  batch_td_kernel<<<sms * 8, B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg, c.row_ptr, c.col);
+  batch_td_kernel<<<sms * blocks_per_sm(batch_td_kernel, B), B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg,
+                                                                      c.row_ptr, c.col);
   if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
-  batch_stats_kernel<<<sms * 2, B, 0, s>>>(bs.ctl, c.mdeg);
-  batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, cond, use_cond);
+  batch_stats_kernel<<<sms * blocks_per_sm(batch_stats_kernel, B), B, 0, s>>>(bs.ctl, c.mdeg);
+  batch_control_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, c.mdeg, cond, use_cond);
 }
 constexpr int kLevelLaunches = 8;
 
@@ -958,6 +993,9 @@ void build_graph(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
   if (bs.graph) cudaGraphDestroy(bs.graph);
   bs.graph_exec = nullptr;
   bs.graph = nullptr;
+  // occupancy queries stay outside the capture
+  blocks_per_sm(batch_td_kernel, 256);
+  blocks_per_sm(batch_stats_kernel, 256);
   check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
   cudaGraph_t cg = nullptr;
   cudaGraph_t body = nullptr;
@@ -972,7 +1010,7 @@ void build_graph(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
     if (err == cudaSuccess)
       err = cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault);
     if (err == cudaSuccess) {
-      batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, batch_csr(g).mdeg, cond, 1);
+      batch_control_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, batch_csr(g).mdeg, cond, 1);
       err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
     }
     cudaGraphNode_t node = nullptr;
@@ -1063,7 +1101,7 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
     launches = 3;  // per level below
   } else {
     launch_prologue(g, bs, s, sms);
-    batch_control_kernel<<<1, 1, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
+    batch_control_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, c.mdeg, 0, 0);
     launches = 3;
   }
   // per level on the host: start, queue built, bottom-up done, top-down done
