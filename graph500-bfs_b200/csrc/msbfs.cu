@@ -603,19 +603,29 @@ struct BatchSetupArg {
   int edgefactor, K;
   long long v[kBatchMax];  // entry vertex of each root (original id)
   int lv[kBatchMax];       // its level
+  // planes[0] is zero except at the rows the previous batch seeded there
+  // (clear[0..nclear)); full_clear when that is not known (new pool, failed
+  // batch)
+  int full_clear, nclear;
+  int clear[kBatchMax];
 };
 
-// seen = 0, planes[0] = 0 and the touched-row bitmap of level 0 = 0.
+// seen = 0, planes[0] = 0 and the touched-row bitmap of level 0 = 0.  Only
+// seeding writes planes[0], so after a batch it holds bits at that batch's
+// level-0 root rows alone, and clearing those rows restores it.
 __global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
   const int64_t n = a->R;
   unsigned long long* __restrict__ seen = a->seen;
   unsigned long long* __restrict__ p0 = a->planes;
   uint32_t* __restrict__ rb = a->rowbits[0];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool full = a->full_clear != 0;
+  for (int64_t i = t0; i < n; i += stride) {
     seen[i] = 0ull;
-    p0[i] = 0ull;
+    if (full) p0[i] = 0ull;
   }
+  if (!full && t0 < a->nclear) p0[a->clear[t0]] = 0ull;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31) >> 5);
        i += stride)
     rb[i] = 0u;
@@ -846,6 +856,8 @@ cudaEvent_t BatchState::event(size_t i) {
 void BatchState::release(DeviceArena& arena) {
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
   ev.clear();
+  plane0_clean = false;
+  plane0_rows.clear();
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (graph) cudaGraphDestroy(graph);
   graph_exec = nullptr;
@@ -1085,6 +1097,10 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
   a.beta = beta;
   a.edgefactor = edgefactor;
   a.K = k;
+  a.full_clear = bs.plane0_clean ? 0 : 1;
+  a.nclear = 0;
+  for (int32_t r : bs.plane0_rows) a.clear[a.nclear++] = r;
+  bs.plane0_clean = false;  // until this batch completes
   bs.K = k;
 
   if (use_graph && (!bs.graph_exec || bs.graph_key != graph_key_of(g, bs, sms)))
@@ -1139,6 +1155,10 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
   const BatchCtl& h = *bs.hctl;
   // the last level found nothing: planes [0, level) hold the levels
   bs.levels = h.level;
+  bs.plane0_rows.clear();
+  for (int i = 0; i < k; ++i)
+    if (h.root_lv[i] == 0 && h.root_row[i] >= 0) bs.plane0_rows.push_back(h.root_row[i]);
+  bs.plane0_clean = true;
   b200bfs_batch_stats r;
   memset(&r, 0, sizeof(r));
   r.num_roots = k;

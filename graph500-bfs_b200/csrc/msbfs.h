@@ -92,6 +92,10 @@ struct BatchState {
   // 64 roots: 8 / 32 / 128 / 1024 probes give 29.0 / 26.2 / 24.3 / 24.6 ms.
   int bu_probe = 128;
   int bu_round = 4;
+  // planes[0] is zero except at plane0_rows (the last batch's level-0 root
+  // rows); false after allocation and while a batch runs
+  bool plane0_clean = false;
+  std::vector<int32_t> plane0_rows;
   int K = 0;
   int64_t levels = 0;                 // planes in use = last level + 1
   std::vector<int64_t> roots;         // original ids
