@@ -602,7 +602,8 @@ def main():
             gbs = nbytes / (ms / 1e3) / 1e9
             kernels[name] = {"ms_per_search": ms / len(stats), "achieved_gbs": gbs,
                              "frac": gbs / peak,
-                             "share_of_search_time": ms / (1e3 * sum(times))}
+                             "share_of_search_time": ms / (1e3 * sum(times)),
+                             "traffic": ncu_traffic(name)}
 
     line = {
         "metric": f"harmonic-mean GTEPS, SCALE {args.scale}; 64-root batched BFS/s + p99 vs 1-root",
