@@ -288,8 +288,11 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * "batch_graph" (1: b200bfs_run_batch runs its level loop as a CUDA graph on
  * the device, 0: the host launches each level and per-level times are
  * recorded), "batch_alpha" (the alpha b200bfs_run_batch uses when given
- * alpha <= 0; default 30).  None of them changes levels or the validity of
- * parents. */
+ * alpha <= 0; default 30), "batch_probe" (4, 8, 16, 32, 64, 128, 256 or
+ * 1024: neighbours a lane of the batched bottom-up sweep probes before the
+ * warp sweeps its row; default 128) and "batch_round" (4 or 8: of them
+ * loaded together; default 4).  None of them changes levels or the validity
+ * of parents. */
 int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value);
 
 /* The CUDA stream (a cudaStream_t) the engine launches its kernels on, for
