@@ -50,6 +50,19 @@ __device__ __forceinline__ unsigned long long* plane_ptr(const BatchCtl* c, long
   return c->planes + L * c->R;
 }
 
+// Zero-fills p[0, n) with 16-byte stores from thread t0 of a grid of
+// `stride` threads (p is 8-byte aligned: a plane starts at L * R words).
+__device__ __forceinline__ void zero_u64(unsigned long long* __restrict__ p, int64_t n,
+                                         int64_t t0, int64_t stride) {
+  const int64_t head = ((uintptr_t)p & 15) ? 1 : 0;
+  if (n <= 0) return;
+  if (head && t0 == 0) p[0] = 0ull;
+  ulonglong2* q = reinterpret_cast<ulonglong2*>(p + head);
+  const int64_t n2 = (n - head) >> 1;
+  for (int64_t i = t0; i < n2; i += stride) q[i] = make_ulonglong2(0ull, 0ull);
+  if (((n - head) & 1) && t0 == 0) p[n - 1] = 0ull;
+}
+
 // Level start: clears the touched-row bitmap of the level and, when no
 // bottom-up sweep will write every row of the level's plane, zero-fills the
 // plane for the top-down push to OR into.
@@ -61,10 +74,9 @@ __global__ void batch_clear_kernel(const BatchCtl* __restrict__ ctl) {
   unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
   const bool zero_plane = !ctl->has_bu;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < W; i += stride) rb[i] = 0u;
-  if (zero_plane)
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < R; i += stride)
-      cur[i] = 0ull;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = t0; i < W; i += stride) rb[i] = 0u;
+  if (zero_plane) zero_u64(cur, R, t0, stride);
 }
 
 // Queue pass 1 (top-down levels): per-block count and degree sum of the rows
@@ -621,10 +633,8 @@ __global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool full = a->full_clear != 0;
-  for (int64_t i = t0; i < n; i += stride) {
-    seen[i] = 0ull;
-    if (full) p0[i] = 0ull;
-  }
+  zero_u64(seen, n, t0, stride);
+  if (full) zero_u64(p0, n, t0, stride);
   if (!full && t0 < a->nclear) p0[a->clear[t0]] = 0ull;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31) >> 5);
        i += stride)
