@@ -147,6 +147,29 @@ def test_batch_long_path_grows_planes(engine):
     assert st.levels == 59
 
 
+def test_consecutive_batches_different_roots(engine, graphs):
+    """Each batch starts from the previous batch's planes: level 0 is cleared
+    only at the rows the previous batch seeded there, so batches over
+    different root sets (and different batch sizes) must not see each
+    other's roots; the probe depth of the sweep must not change levels."""
+    edges, g = graphs(16)
+    engine.generate_graph(16, 16)
+    engine.prepare(16)
+    he = g.has_edge()
+    sets = [O.find_roots(he, 1 << 16, 64, 7), O.find_roots(he, 1 << 16, 9, 8),
+            O.find_roots(he, 1 << 16, 33, 9)]
+    try:
+        for probe, roots in zip((4, 128, 1024), sets):
+            engine.set_option("batch_probe", probe)
+            roots = [int(r) for r in roots]
+            engine.run_batch(roots)
+            for i in (0, len(roots) // 2, len(roots) - 1):
+                engine.batch_select(i)
+                assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(roots[i])), (probe, i)
+    finally:
+        engine.set_option("batch_probe", 128)
+
+
 def test_batch_then_single_root(engine, graphs):
     edges, g = graphs(14)
     engine.generate_graph(14, 16)
