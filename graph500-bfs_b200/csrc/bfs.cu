@@ -20,6 +20,7 @@
 //       turn the new bitmap bits into the next queue with its degree prefix;
 //   direction switch (:3413-3457)  -> host, from the per-level counters.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include "common.cuh"
 #include "bfs_internal.h"
@@ -678,7 +679,9 @@ __device__ __forceinline__ void td_chunk_body(
 // kDeg: also the per-block CSR degree sums of the frontier, which only a
 // following top-down level needs (its queue's degree prefix); after a
 // top-down level they are computed by frontier_deg_body once the next
-// direction is known.
+// direction is known.  The level counters (nq, nq_edges) are added only
+// after a top-down level: with kDeg the pass rebuilds the queue of a
+// bottom-up level whose counters the bottom-up kernel already reported.
 template <bool kDeg>
 __device__ __forceinline__ void frontier_count_body(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
@@ -723,7 +726,7 @@ __device__ __forceinline__ void frontier_count_body(
     }
     blk_cnt[blockIdx.x] = A;
     if (kDeg) blk_deg[blockIdx.x] = Bs;
-    if (A) {
+    if (A && !kDeg) {
       atomicAdd(&ctr->nq, (unsigned long long)A);
       atomicAdd(&ctr->nq_edges, (unsigned long long)C);
     }
@@ -913,10 +916,18 @@ __global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
   frontier_write_body(fr, W, row_ptr, blk_cnt, blk_deg, queue, qdeg);
 }
 
-__global__ void clear_counters_kernel(Counters* ctr) {
+// End of a level: the counters go to host-mapped memory, then the level's
+// sequence number (after a system-wide fence, so the host that sees the
+// number sees the counters); the per-level sums are cleared for the next
+// level, which runs after this kernel in stream order.
+__global__ void publish_kernel(Counters* __restrict__ ctr, BfsState::Published* pub,
+                               unsigned long long seq) {
+  pub->c = *ctr;
   ctr->nq = 0;
   ctr->nq_edges = 0;
   ctr->scanned = 0;
+  __threadfence_system();
+  *(volatile unsigned long long*)&pub->seq = seq;
 }
 
 __global__ void levels_kernel(const int64_t* __restrict__ pred, int64_t n,
@@ -1210,7 +1221,10 @@ void BfsState::allocate(DeviceArena& arena, const Graph& g) {
   blk_deg = arena_alloc<int64_t>(arena, nblk + 1, "block degrees");
   pred = arena_alloc<int64_t>(arena, pred_size + 2, "pred");
   ctr = arena_alloc<Counters>(arena, 1, "counters");
-  check_cuda(cudaMallocHost(&hctr, sizeof(Counters)), "pinned counters");
+  check_cuda(cudaHostAlloc(&hpub, sizeof(Published), cudaHostAllocMapped), "mapped counters");
+  check_cuda(cudaHostGetDevicePointer(&dpub, hpub, 0), "mapped counters");
+  hpub->seq = 0;
+  pub_seq = 0;
   sctl = arena_alloc<SingleCtl>(arena, 1, "search control block");
   sarg = arena_alloc<SgArg>(arena, 1, "search arguments");
   d_vis = arena_alloc<uint32_t*>(arena, 2, "bitmap pointers");
@@ -1264,8 +1278,9 @@ void BfsState::release(DeviceArena& arena) {
   if (pmap) arena.free(pmap);
   rp = nullptr;
   pmap = nullptr;
-  cudaFreeHost(hctr);
-  hctr = nullptr;
+  if (hpub) cudaFreeHost(hpub);
+  hpub = nullptr;
+  dpub = nullptr;
   allocated = false;
 }
 
@@ -1389,6 +1404,7 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   const bool bu_first = opt.bu_first != 0;
   const bool assemble = use_pred_assembly(g, opt);
   if (assemble && !st.pmap) throw Error{B200BFS_ERR_STATE, "pred assembly map not built"};
+  st.asm_ev = -1;  // the graph does not time the assembly pass
   if (!st.sgexec ||
       st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction, bu_first, assemble))
     sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction, bu_first, assemble);
@@ -1447,6 +1463,30 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
 
 }  // namespace
 
+// Publishes the level's counters and waits for them: polls the host-mapped
+// sequence number, checking the stream every few thousand polls so that a
+// failed kernel ends the wait with its error instead of a hang.
+static Counters wait_level(BfsState& st, cudaStream_t s) {
+  const unsigned long long seq = ++st.pub_seq;
+  publish_kernel<<<1, 1, 0, s>>>(st.ctr, st.dpub, seq);
+  check_cuda(cudaGetLastError(), "publish");
+  volatile unsigned long long* flag = &st.hpub->seq;
+  for (unsigned long long n = 1; *flag != seq; ++n) {
+    if ((n & 4095) == 0) {
+      const cudaError_t e = cudaStreamQuery(s);
+      if (e == cudaSuccess) {
+        if (*flag != seq) throw Error{B200BFS_ERR_CUDA, "level counters not published"};
+        break;
+      }
+      if (e != cudaErrorNotReady) check_cuda(e, "level");
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  Counters h;
+  memcpy(&h, (const void*)&st.hpub->c, sizeof(Counters));
+  return h;
+}
+
 // The level loop with the reference's direction switch.
 void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                   int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
@@ -1497,8 +1537,6 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     if (at) at[8] = level;  // AUTO_LEVEL
     const int64_t prev_nq = global_nq_size;
     forward = next_forward;
-    clear_counters_kernel<<<1, 1, 0, s>>>(st.ctr);
-    ++launches;
     int64_t frontier_in = 0;
     check_cuda(cudaEventRecord(st.event(nev), s), "event");
     timed.push_back({forward, nev});
@@ -1563,10 +1601,8 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       launches += 1;
       cur ^= 1;
     }
-    check_cuda(cudaMemcpyAsync(st.hctr, st.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s),
-               "counters");
-    check_cuda(cudaStreamSynchronize(s), "level");
-    const Counters h = *st.hctr;
+    const Counters h = wait_level(st, s);
+    ++launches;
     global_nq_size = (int64_t)h.nq;
     if (forward) {
       global_nq_edges = (int64_t)h.nq_edges;
@@ -1663,17 +1699,20 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     (t.first ? rs.td_ms : rs.bu_ms) += ms;
     if (k < st.levels.size()) st.levels[k].ms = ms;
   }
-  if (assemble) {
-    float ms = 0;
-    check_cuda(cudaEventSynchronize(st.ev[nev - 1]), "assembly");
-    check_cuda(cudaEventElapsedTime(&ms, st.ev[nev - 2], st.ev[nev - 1]), "elapsed");
-    rs.pred_ms = ms;
-  }
+  st.asm_ev = assemble ? (int)(nev - 2) : -1;  // read by finish_run_stats
   rs.kernel_launches = launches;
   rs.levels = (int32_t)level;
   rs.visited = visited;
   rs.algorithmic_bytes = bytes;
   if (stats) *stats = rs;
+}
+
+void finish_run_stats(BfsState& st, b200bfs_run_stats* stats) {
+  if (!stats || st.asm_ev < 0) return;
+  float ms = 0;
+  check_cuda(cudaEventSynchronize(st.ev[st.asm_ev + 1]), "assembly");
+  check_cuda(cudaEventElapsedTime(&ms, st.ev[st.asm_ev], st.ev[st.asm_ev + 1]), "elapsed");
+  stats->pred_ms = ms;
 }
 
 void levels_from_pred(const BfsState& st, cudaStream_t s, int sms, int32_t* d_levels) {

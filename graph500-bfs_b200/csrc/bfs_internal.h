@@ -53,7 +53,18 @@ struct BfsState {
   int64_t* blk_deg = nullptr;
   int64_t* pred = nullptr;                // [pred_size], original ids
   Counters* ctr = nullptr;
-  Counters* hctr = nullptr;               // pinned mirror
+  // The level counters as the device publishes them at the end of a level,
+  // in host-mapped memory (hpub; dpub is its device address), with the
+  // level's sequence number written last; the host waits for it by polling
+  // instead of a copy and a stream synchronisation.
+  struct Published {
+    Counters c;
+    unsigned long long seq;
+  };
+  Published* hpub = nullptr;
+  Published* dpub = nullptr;
+  unsigned long long pub_seq = 0;
+  int asm_ev = -1;                        // event pair of the last assembly pass
   std::vector<cudaEvent_t> ev;            // per-level kernel timing events
   std::vector<b200bfs_level_stats> levels;  // per-level record of the last search
   // pred holds exactly the last search's result (-1 everywhere else), so the
@@ -127,5 +138,7 @@ inline bool use_pred_assembly(const Graph&, const RunOptions& o) { return o.pred
 void build_pred_assembly(DeviceArena& arena, const Graph& g, BfsState& st, cudaStream_t s,
                          int sms);
 int64_t assembly_bytes(const BfsState& st, int64_t visited);
+// After the search's stream work is complete: the assembly pass time.
+void finish_run_stats(BfsState& st, b200bfs_run_stats* stats);
 
 }  // namespace b200bfs

@@ -157,6 +157,8 @@ int b200bfs_create(const b200bfs_config* cfg, b200bfs_handle** out) {
     b200bfs::check_cuda(cudaGetDeviceProperties(&prop, dev), "device properties");
     e.sms = prop.multiProcessorCount;
     b200bfs::check_cuda(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking), "stream");
+    b200bfs::check_cuda(cudaEventCreate(&e.run_ev[0]), "event");
+    b200bfs::check_cuda(cudaEventCreate(&e.run_ev[1]), "event");
   });
   if (rc != B200BFS_OK) {
     delete h;
@@ -170,6 +172,8 @@ int b200bfs_destroy(b200bfs_handle* h) {
   if (!h) return B200BFS_ERR_INVALID;
   guarded(h, [&](Engine& e) {
     e.free_graph();
+    for (cudaEvent_t& ev : e.run_ev)
+      if (ev) cudaEventDestroy(ev);
     if (e.stream) cudaStreamDestroy(e.stream);
     e.stream = nullptr;
   });
@@ -424,10 +428,7 @@ int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha, d
     require(e.prepared, B200BFS_ERR_STATE, "prepare_bfs not called");
     require(root >= 0 && root < e.g.nverts, B200BFS_ERR_INVALID, "root out of range");
     require(alpha > 0 && beta > 0 && edgefactor > 0, B200BFS_ERR_INVALID, "bad parameters");
-    cudaEvent_t t0, t1;
-    b200bfs::check_cuda(cudaEventCreate(&t0), "event");
-    b200bfs::check_cuda(cudaEventCreate(&t1), "event");
-    b200bfs::check_cuda(cudaEventRecord(t0, e.stream), "event");
+    b200bfs::check_cuda(cudaEventRecord(e.run_ev[0], e.stream), "event");
     b200bfs_run_stats rs;
     if (e.g.core.enabled)
       b200bfs::core_run_bfs(e.g, e.st, e.stream, e.sms, root, edgefactor, alpha, beta, at, e.opt,
@@ -435,12 +436,11 @@ int b200bfs_run(b200bfs_handle* h, int64_t root, int edgefactor, double alpha, d
     else
       b200bfs::run_bfs_core(e.g, e.st, e.stream, e.sms, root, 0, edgefactor, alpha, beta, at,
                             e.opt, &rs);
-    b200bfs::check_cuda(cudaEventRecord(t1, e.stream), "event");
-    b200bfs::check_cuda(cudaEventSynchronize(t1), "run");
+    b200bfs::check_cuda(cudaEventRecord(e.run_ev[1], e.stream), "event");
+    b200bfs::check_cuda(cudaEventSynchronize(e.run_ev[1]), "run");
     float ms = 0;
-    cudaEventElapsedTime(&ms, t0, t1);
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    cudaEventElapsedTime(&ms, e.run_ev[0], e.run_ev[1]);
+    b200bfs::finish_run_stats(e.st, &rs);
     rs.device_ms = ms;
     e.last_stats = rs;
     e.have_run = true;

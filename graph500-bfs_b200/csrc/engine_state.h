@@ -13,6 +13,7 @@ struct Engine {
   int device = 0;
   int sms = 148;
   cudaStream_t stream = nullptr;
+  cudaEvent_t run_ev[2] = {nullptr, nullptr};  // b200bfs_run start / end
   DeviceArena arena;
   Graph g;
   BfsState st;
