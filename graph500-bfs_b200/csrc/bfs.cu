@@ -28,7 +28,11 @@
 namespace b200bfs {
 namespace {
 
-constexpr int kWordsPerBlock = 256;  // frontier kernels: one thread per word
+// frontier kernels: a thread handles kWordsPerThread consecutive bitmap
+// words (one 16-byte load), a block kWordsPerBlock
+constexpr int kFrontierThreads = 256;
+constexpr int kWordsPerThread = 4;
+constexpr int kWordsPerBlock = kFrontierThreads * kWordsPerThread;
 constexpr int kTdTile = 256;         // adjacency entries per warp tile
 
 __device__ __forceinline__ void warp_inclusive_scan2(int64_t& a, int64_t& b) {
@@ -682,26 +686,48 @@ __device__ __forceinline__ void td_chunk_body(
 // direction is known.  The level counters (nq, nq_edges) are added only
 // after a top-down level: with kDeg the pass rebuilds the queue of a
 // bottom-up level whose counters the bottom-up kernel already reported.
+// The kWordsPerThread words of thread t of the block (words at or beyond W
+// read as 0; the bitmaps are allocated with 4 words of padding).
+__device__ __forceinline__ int64_t frontier_word0() {
+  return ((int64_t)blockIdx.x * kFrontierThreads + threadIdx.x) * kWordsPerThread;
+}
+__device__ __forceinline__ void load_words(const uint32_t* __restrict__ p, int64_t w0, int64_t W,
+                                           uint32_t (&x)[kWordsPerThread]) {
+  const uint4 v = w0 < W ? *reinterpret_cast<const uint4*>(p + w0) : make_uint4(0, 0, 0, 0);
+  x[0] = v.x;
+  x[1] = w0 + 1 < W ? v.y : 0u;
+  x[2] = w0 + 2 < W ? v.z : 0u;
+  x[3] = w0 + 3 < W ? v.w : 0u;
+}
+
 template <bool kDeg>
 __device__ __forceinline__ void frontier_count_body(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
     int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
-  __shared__ int64_t s_a[kWordsPerBlock / 32], s_b[kWordsPerBlock / 32], s_c[kWordsPerBlock / 32];
-  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
+  __shared__ int64_t s_a[kFrontierThreads / 32], s_b[kFrontierThreads / 32],
+      s_c[kFrontierThreads / 32];
+  const int64_t w0 = frontier_word0();
   int64_t cnt = 0, dsum = 0, msum = 0;
-  if (w < W) {
-    const uint32_t a = nw[w];
-    uint32_t f = a & ~old[w];
-    fr[w] = f;
-    old[w] = a;
-    cnt = __popc(f);
-    while (f) {
-      const int bpos = __ffs(f) - 1;
-      f &= f - 1;
-      const int64_t v = w * 32 + bpos;
-      if (kDeg) dsum += row_ptr[v + 1] - row_ptr[v];
-      msum += mdeg[v];
+  if (w0 < W) {
+    uint32_t a[kWordsPerThread], o[kWordsPerThread];
+    load_words(nw, w0, W, a);
+    load_words(old, w0, W, o);
+    uint32_t f[kWordsPerThread];
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) f[k] = a[k] & ~o[k];
+    *reinterpret_cast<uint4*>(fr + w0) = make_uint4(f[0], f[1], f[2], f[3]);
+    *reinterpret_cast<uint4*>(old + w0) = make_uint4(a[0], a[1], a[2], a[3]);
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) {
+      cnt += __popc(f[k]);
+      uint32_t g = f[k];
+      while (g) {
+        const int64_t v = (w0 + k) * 32 + __ffs(g) - 1;
+        g &= g - 1;
+        if (kDeg) dsum += row_ptr[v + 1] - row_ptr[v];
+        msum += mdeg[v];
+      }
     }
   }
 #pragma unroll
@@ -719,7 +745,7 @@ __device__ __forceinline__ void frontier_count_body(
   __syncthreads();
   if (threadIdx.x == 0) {
     int64_t A = 0, Bs = 0, C = 0;
-    for (int i = 0; i < kWordsPerBlock / 32; ++i) {
+    for (int i = 0; i < kFrontierThreads / 32; ++i) {
       A += s_a[i];
       Bs += s_b[i];
       C += s_c[i];
@@ -737,15 +763,20 @@ __device__ __forceinline__ void frontier_count_body(
 __device__ __forceinline__ void frontier_deg_body(const uint32_t* __restrict__ fr, int64_t W,
                                                   const int64_t* __restrict__ row_ptr,
                                                   int64_t* __restrict__ blk_deg) {
-  __shared__ int64_t s_b[kWordsPerBlock / 32];
-  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
+  __shared__ int64_t s_b[kFrontierThreads / 32];
+  const int64_t w0 = frontier_word0();
   int64_t dsum = 0;
-  if (w < W) {
-    uint32_t f = fr[w];
-    while (f) {
-      const int64_t v = w * 32 + __ffs(f) - 1;
-      f &= f - 1;
-      dsum += row_ptr[v + 1] - row_ptr[v];
+  if (w0 < W) {
+    uint32_t f[kWordsPerThread];
+    load_words(fr, w0, W, f);
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) {
+      uint32_t g = f[k];
+      while (g) {
+        const int64_t v = (w0 + k) * 32 + __ffs(g) - 1;
+        g &= g - 1;
+        dsum += row_ptr[v + 1] - row_ptr[v];
+      }
     }
   }
 #pragma unroll
@@ -754,7 +785,7 @@ __device__ __forceinline__ void frontier_deg_body(const uint32_t* __restrict__ f
   __syncthreads();
   if (threadIdx.x == 0) {
     int64_t b = 0;
-    for (int i = 0; i < kWordsPerBlock / 32; ++i) b += s_b[i];
+    for (int i = 0; i < kFrontierThreads / 32; ++i) b += s_b[i];
     blk_deg[blockIdx.x] = b;
   }
 }
@@ -810,16 +841,18 @@ __device__ __forceinline__ void frontier_write_body(
     const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
     int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
-  __shared__ int64_t s_a[kWordsPerBlock / 32], s_b[kWordsPerBlock / 32];
-  const int64_t w = (int64_t)blockIdx.x * kWordsPerBlock + threadIdx.x;
-  uint32_t f = (w < W) ? fr[w] : 0u;
-  int64_t cnt = __popc(f), dsum = 0;
-  {
-    uint32_t g = f;
+  __shared__ int64_t s_a[kFrontierThreads / 32], s_b[kFrontierThreads / 32];
+  const int64_t w0 = frontier_word0();
+  uint32_t f[kWordsPerThread] = {0u, 0u, 0u, 0u};
+  if (w0 < W) load_words(fr, w0, W, f);
+  int64_t cnt = 0, dsum = 0;
+#pragma unroll
+  for (int k = 0; k < kWordsPerThread; ++k) {
+    cnt += __popc(f[k]);
+    uint32_t g = f[k];
     while (g) {
-      const int bpos = __ffs(g) - 1;
+      const int64_t v = (w0 + k) * 32 + __ffs(g) - 1;
       g &= g - 1;
-      const int64_t v = w * 32 + bpos;
       dsum += row_ptr[v + 1] - row_ptr[v];
     }
   }
@@ -833,7 +866,7 @@ __device__ __forceinline__ void frontier_write_body(
   __syncthreads();
   if (threadIdx.x == 0) {
     int64_t ra = 0, rb = 0;
-    for (int i = 0; i < kWordsPerBlock / 32; ++i) {
+    for (int i = 0; i < kFrontierThreads / 32; ++i) {
       const int64_t xa = s_a[i], xb = s_b[i];
       s_a[i] = ra;
       s_b[i] = rb;
@@ -844,14 +877,17 @@ __device__ __forceinline__ void frontier_write_body(
   __syncthreads();
   int64_t pos = blk_cnt[blockIdx.x] + s_a[wid] + ic - cnt;
   int64_t dpos = blk_deg[blockIdx.x] + s_b[wid] + id - dsum;
-  while (f) {
-    const int bpos = __ffs(f) - 1;
-    f &= f - 1;
-    const int64_t v = w * 32 + bpos;
-    queue[pos] = (int32_t)v;
-    qdeg[pos] = dpos;
-    ++pos;
-    dpos += row_ptr[v + 1] - row_ptr[v];
+#pragma unroll
+  for (int k = 0; k < kWordsPerThread; ++k) {
+    uint32_t g = f[k];
+    while (g) {
+      const int64_t v = (w0 + k) * 32 + __ffs(g) - 1;
+      g &= g - 1;
+      queue[pos] = (int32_t)v;
+      qdeg[pos] = dpos;
+      ++pos;
+      dpos += row_ptr[v + 1] - row_ptr[v];
+    }
   }
 }
 
@@ -888,14 +924,14 @@ __global__ void __launch_bounds__(256) td_chunk_kernel(
 }
 
 template <bool kDeg>
-__global__ void __launch_bounds__(kWordsPerBlock) frontier_count_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) frontier_count_kernel(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
     int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
   frontier_count_body<kDeg>(nw, old, fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
 }
 
-__global__ void __launch_bounds__(kWordsPerBlock) frontier_deg_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) frontier_deg_kernel(
     const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
     int64_t* __restrict__ blk_deg) {
   frontier_deg_body(fr, W, row_ptr, blk_deg);
@@ -909,7 +945,7 @@ __global__ void __launch_bounds__(1024) frontier_scan_kernel(int64_t* __restrict
   frontier_scan_body(blk_cnt, blk_deg, nblk, qdeg, ctr);
 }
 
-__global__ void __launch_bounds__(kWordsPerBlock) frontier_write_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) frontier_write_kernel(
     const uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
     int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
@@ -1060,7 +1096,7 @@ __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
 // kAfterBu = false: after a top-down level; true: after a bottom-up level
 // whose next level is top-down (the bitmaps have swapped by then).
 template <bool kAfterBu>
-__global__ void __launch_bounds__(kWordsPerBlock) sg_count_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) sg_count_kernel(
     const SingleCtl* __restrict__ c, uint32_t* const* __restrict__ vis_pp,
     uint32_t* __restrict__ fr, int64_t W, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ mdeg, int64_t* __restrict__ blk_cnt,
@@ -1074,7 +1110,7 @@ __global__ void __launch_bounds__(kWordsPerBlock) sg_count_kernel(
 
 // After a top-down level whose next level is top-down: the queue's degree
 // sums.
-__global__ void __launch_bounds__(kWordsPerBlock) sg_deg_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) sg_deg_kernel(
     const SingleCtl* __restrict__ c, const uint32_t* __restrict__ fr, int64_t W,
     const int64_t* __restrict__ row_ptr, int64_t* __restrict__ blk_deg) {
   if (c->done || !c->forward || !c->next_forward) return;
@@ -1090,7 +1126,7 @@ __global__ void __launch_bounds__(1024) sg_scan_kernel(const SingleCtl* __restri
   frontier_scan_body(blk_cnt, blk_deg, nblk, qdeg, ctr);
 }
 
-__global__ void __launch_bounds__(kWordsPerBlock) sg_write_kernel(
+__global__ void __launch_bounds__(kFrontierThreads) sg_write_kernel(
     const SingleCtl* __restrict__ c, const uint32_t* __restrict__ fr, int64_t W,
     const int64_t* __restrict__ row_ptr, const int64_t* __restrict__ blk_cnt,
     const int64_t* __restrict__ blk_deg, int32_t* __restrict__ queue,
@@ -1307,17 +1343,17 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
                                                              st.d_vis, out);
   (bu_first && c.first ? sg_bu_kernel<true> : sg_bu_kernel<false>)<<<sms * 4, B, 0, s>>>(
       st.sctl, st.W, c.row_ptr, c.col, c.first, c.first_inv, c.inv, pidx, st.d_vis, out, st.ctr);
-  sg_count_kernel<false><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
+  sg_count_kernel<false><<<nblk, kFrontierThreads, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                          c.row_ptr, c.mdeg, st.blk_cnt,
                                                          st.blk_deg, st.ctr);
   sg_control_kernel<<<1, 1, 0, s>>>(st.sctl, st.sarg, st.ctr, st.R, st.W, c.nedges, c.nrows,
                                     force_direction, cond);
-  sg_count_kernel<true><<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
+  sg_count_kernel<true><<<nblk, kFrontierThreads, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                         c.row_ptr, c.mdeg, st.blk_cnt,
                                                         st.blk_deg, st.ctr);
-  sg_deg_kernel<<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_deg);
+  sg_deg_kernel<<<nblk, kFrontierThreads, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_deg);
   sg_scan_kernel<<<1, 1024, 0, s>>>(st.sctl, st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
-  sg_write_kernel<<<nblk, kWordsPerBlock, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_cnt,
+  sg_write_kernel<<<nblk, kFrontierThreads, 0, s>>>(st.sctl, st.fr, st.W, c.row_ptr, st.blk_cnt,
                                                   st.blk_deg, st.queue, st.qdeg);
 }
 constexpr int kSgLevelLaunches = 12;
@@ -1568,7 +1604,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
         launch_td(td_wide_kernel, 0);
       check_cuda(cudaEventRecord(st.event(nev - 1), s), "event");
       launches += 2;
-      frontier_count_kernel<false><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+      frontier_count_kernel<false><<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(
           st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
           st.ctr);
       frontier_in = qsize;
@@ -1661,14 +1697,14 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     if (next_forward) {
       // Build the next queue from the bits set in this level.
       if (!forward)  // after bottom-up: bits of vis[cur] not in vis[cur^1]
-        frontier_count_kernel<true><<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+        frontier_count_kernel<true><<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(
             st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
             st.ctr);
       else  // after top-down: the counts are there, the degree sums not yet
-        frontier_deg_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(st.fr, st.W, c.row_ptr,
+        frontier_deg_kernel<<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(st.fr, st.W, c.row_ptr,
                                                                          st.blk_deg);
       frontier_scan_kernel<<<1, 1024, 0, s>>>(st.blk_cnt, st.blk_deg, st.nblk, st.qdeg, st.ctr);
-      frontier_write_kernel<<<(unsigned)st.nblk, kWordsPerBlock, 0, s>>>(
+      frontier_write_kernel<<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(
           st.fr, st.W, c.row_ptr, st.blk_cnt, st.blk_deg, st.queue, st.qdeg);
       launches += 3;
       qsize = global_nq_size;
