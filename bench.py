@@ -54,6 +54,9 @@ def parse():
                    help="without the -A alpha/beta tuner")
     p.add_argument("--no-tune-engine", dest="tune_engine", action="store_false",
                    help="keep the default kernel forms and batch alpha instead of timing them")
+    p.add_argument("--no-tune-switch", dest="tune_switch", action="store_false",
+                   help="keep alpha/beta as given (or as -A tuned them) instead of refining "
+                        "them by timing in the engine tuner")
     p.add_argument("--batch-roots", type=int, default=64)
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--batch-alpha", type=float, default=0.0,
@@ -429,6 +432,7 @@ def workload_config(args):
             "scale": args.scale, "edgefactor": args.edgefactor, "roots": args.roots,
             "corebfs": bool(args.corebfs), "group_reorder": bool(args.group_reorder),
             "alpha": args.alpha, "beta": args.beta,
+            "alpha_beta_before_engine_tuner": getattr(args, "alpha_beta_given", None),
             "l2": "inputs larger than L2 (device CSR of tens of GB, pred re-initialised "
                   "every search)",
             "parallelism": "replicas"}
@@ -517,7 +521,13 @@ def main():
     tuner = None
     if args.tune_engine:
         t0 = time.time()
-        tuner = eng.tune_engine(roots, args.edgefactor, args.alpha, args.beta).as_dict()
+        what = b200bfs.TUNE_FORMS | b200bfs.TUNE_BATCH_ALPHA
+        if args.tune_switch:
+            what |= b200bfs.TUNE_SWITCH
+        tuner = eng.tune_engine(roots, args.edgefactor, args.alpha, args.beta, what).as_dict()
+        if args.tune_switch:
+            args.alpha_beta_given = [args.alpha, args.beta]
+            args.alpha, args.beta = tuner["alpha"], tuner["beta"]
         log(f"[rank {rank}] engine tuner: {tuner} ({time.time() - t0:.1f}s)")
 
     stream = torch.cuda.ExternalStream(eng.stream())

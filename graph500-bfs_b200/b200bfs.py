@@ -105,14 +105,15 @@ class BatchStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
-TUNE_FORMS, TUNE_BATCH_ALPHA = 1, 2
+TUNE_FORMS, TUNE_BATCH_ALPHA, TUNE_SWITCH = 1, 2, 4
 
 
 class TuneReport(ctypes.Structure):
     _fields_ = [("bu_kernel", ctypes.c_int32), ("td_kernel", ctypes.c_int32),
                 ("batch_alpha", ctypes.c_double), ("single_ms", ctypes.c_double),
                 ("batch_ms", ctypes.c_double), ("searches", ctypes.c_int32),
-                ("batches", ctypes.c_int32)]
+                ("batches", ctypes.c_int32), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

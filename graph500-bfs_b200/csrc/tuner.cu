@@ -97,6 +97,29 @@ extern "C" int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int 
       e.opt.td_kernel = best_td;
       rep.single_ms = best / (double)rs.size();
     }
+    rep.alpha = alpha;
+    rep.beta = beta;
+    if (what & B200BFS_TUNE_SWITCH) {
+      // coordinate search: alpha, then beta, each scaled by a few factors
+      double best = b200bfs::time_searches(e, rs, edgefactor, alpha, beta, ev);
+      rep.searches += (int)rs.size() + 1;
+      for (int param = 0; param < 2; ++param) {
+        const double base = param == 0 ? rep.alpha : rep.beta;
+        double pick = base;
+        for (double f : {0.5, 0.7, 1.4, 2.0}) {
+          const double a = param == 0 ? base * f : rep.alpha;
+          const double b = param == 1 ? base * f : rep.beta;
+          const double t = b200bfs::time_searches(e, rs, edgefactor, a, b, ev);
+          rep.searches += (int)rs.size() + 1;
+          if (t < 0.99 * best) {
+            best = t;
+            pick = base * f;
+          }
+        }
+        (param == 0 ? rep.alpha : rep.beta) = pick;
+      }
+      rep.single_ms = best / (double)rs.size();
+    }
     if (what & B200BFS_TUNE_BATCH_ALPHA) {
       b200bfs::ensure_batch_view(e.arena, e.g, e.stream, e.sms);
       const int k = std::min(num_roots, B200BFS_BATCH_MAX);

@@ -247,7 +247,8 @@ int b200bfs_get_run_stats(b200bfs_handle* h, b200bfs_run_stats* out);
 
 enum {
   B200BFS_TUNE_FORMS = 1 << 0,        /* bottom-up and top-down kernel forms   */
-  B200BFS_TUNE_BATCH_ALPHA = 1 << 1   /* alpha of b200bfs_run_batch            */
+  B200BFS_TUNE_BATCH_ALPHA = 1 << 1,  /* alpha of b200bfs_run_batch            */
+  B200BFS_TUNE_SWITCH = 1 << 2        /* single-source alpha/beta, refined     */
 };
 
 typedef struct b200bfs_tune_report {
@@ -258,6 +259,8 @@ typedef struct b200bfs_tune_report {
   double batch_ms;               /* batch time with the chosen alpha          */
   int32_t searches;              /* single-source searches the tuner ran      */
   int32_t batches;               /* batches the tuner ran                     */
+  double alpha, beta;            /* single-source switch parameters: refined
+                                    with B200BFS_TUNE_SWITCH, else the input   */
 } b200bfs_tune_report;
 
 /* No counterpart in the reference, whose equivalents are compile-time
@@ -265,8 +268,13 @@ typedef struct b200bfs_tune_report {
  * and top-down kernel forms (timing each on up to 16 of the roots with
  * alpha/beta) and the batched search's alpha (timing 64-root batches with
  * 10..400), and keeps the fastest in the engine's options ("bu_kernel",
- * "td_kernel", "batch_alpha").  what: B200BFS_TUNE_* bits.  Levels and
- * parent validity do not depend on the choices.  out may be NULL. */
+ * "td_kernel", "batch_alpha").  With B200BFS_TUNE_SWITCH it also refines
+ * the given alpha/beta (for instance the -A tuner's) by timing the same
+ * searches with each scaled by 0.5, 0.7, 1.4 and 2, one after the other,
+ * keeping a change only when it is more than 1 % faster; the result is
+ * returned in out->alpha / out->beta for the caller to pass to b200bfs_run.
+ * what: B200BFS_TUNE_* bits.  Levels and parent validity do not depend on
+ * the choices.  out may be NULL. */
 int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, int edgefactor,
                         double alpha, double beta, int what, b200bfs_tune_report* out);
 

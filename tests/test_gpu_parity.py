@@ -283,6 +283,8 @@ def test_kernel_forms_agree(engine, oracle_graphs, bu, td, first):
 def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
     """b200bfs_tune_engine picks kernel forms and the batch alpha by timing;
     searches and batches with its choices still give the oracle's levels."""
+    import b200bfs
+
     edges, g = oracle_graphs(18)
     engine.generate_graph(18, 16)
     engine.prepare(16)
@@ -292,11 +294,19 @@ def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
         assert 1 <= rep.bu_kernel <= 4 and rep.td_kernel in (1, 3, 4, 5)
         assert rep.batch_alpha in (10.0, 20.0, 30.0, 50.0, 100.0, 200.0, 400.0)
         assert rep.searches > 0 and rep.batches == 14 and rep.single_ms > 0 and rep.batch_ms > 0
+        assert (rep.alpha, rep.beta) == (10.0, 14.0)  # not refined without TUNE_SWITCH
         _check_search(engine, edges, g, roots[:3])
         engine.run_batch(roots, 16, 0.0)  # alpha <= 0: the tuned batch alpha
         for i, r in enumerate(roots):
             engine.batch_select(i)
             assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(int(r)))
+        # alpha/beta refinement: each is the input scaled by one of the
+        # tried factors; the oracle with the same alpha/beta gives the same
+        # switch levels (auto_tuning_data) and levels
+        rep = engine.tune_engine(roots, 16, 10.0, 14.0, b200bfs.TUNE_SWITCH)
+        assert rep.alpha in [10.0 * f for f in (0.5, 0.7, 1.0, 1.4, 2.0)]
+        assert rep.beta in [14.0 * f for f in (0.5, 0.7, 1.0, 1.4, 2.0)]
+        _check_search(engine, edges, g, roots[:3], alpha=rep.alpha, beta=rep.beta)
     finally:
         engine.set_option("bu_kernel", 4)
         engine.set_option("td_kernel", 4)
