@@ -270,6 +270,40 @@ __device__ __forceinline__ void td_expand_body(
 
 // Bottom-up step.  cur is the visited bitmap before this level (read-only
 // here); nxt receives cur | newly found bits for every word.
+// End of the last kernel of a level (pub null: not the last one).  The
+// last block to finish publishes the level: the counters go to host-mapped
+// memory, then the level's sequence number (after a system-wide fence, so
+// the host that sees the number sees the counters), and the per-level sums
+// are cleared for the next level, which runs after this kernel in stream
+// order.  Every block's counter atomics come before its ticket (fence); the
+// last ticket holder reads the totals after a second fence.
+__device__ __forceinline__ void publish_if_last(Counters* __restrict__ ctr,
+                                                BfsState::Published* pub,
+                                                unsigned long long seq) {
+  if (!pub) return;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  __threadfence();
+  if (atomicAdd(&ctr->blocks_done, 1u) != gridDim.x - 1) return;
+  __threadfence();
+  volatile Counters* vc = ctr;
+  Counters c;
+  c.nq = vc->nq;
+  c.nq_edges = vc->nq_edges;
+  c.scanned = vc->scanned;
+  c.qsize = vc->qsize;
+  c.qedges = vc->qedges;
+  c.error = vc->error;
+  c.blocks_done = 0;
+  pub->c = c;
+  ctr->nq = 0;
+  ctr->nq_edges = 0;
+  ctr->scanned = 0;
+  ctr->blocks_done = 0;
+  __threadfence_system();
+  *(volatile unsigned long long*)&pub->seq = seq;
+}
+
 template <int kProbe>
 __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cur,
                                                  uint32_t* __restrict__ nxt, int64_t W,
@@ -278,7 +312,9 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
                                                  const int32_t* __restrict__ inv,
     const int32_t* __restrict__ pidx,
                                                  int64_t* __restrict__ pred, int64_t level,
-                                                 Counters* __restrict__ ctr) {
+                                                 Counters* __restrict__ ctr,
+                                                 BfsState::Published* pub,
+                                                 unsigned long long seq) {
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -345,6 +381,7 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
     if (found_total) atomicAdd(&ctr->nq, found_total);
     if (scanned) atomicAdd(&ctr->scanned, scanned);
   }
+  publish_if_last(ctr, pub, seq);
 }
 
 // Bottom-up step, second form: a warp step covers kWords bitmap words, so
@@ -909,9 +946,11 @@ __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
     const int32_t* __restrict__ first, const int32_t* __restrict__ finv,
     const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
-    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
+    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr,
+    BfsState::Published* pub, unsigned long long seq) {
   bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred, level,
                                ctr);
+  publish_if_last(ctr, pub, seq);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
@@ -927,8 +966,10 @@ template <bool kDeg>
 __global__ void __launch_bounds__(kFrontierThreads) frontier_count_kernel(
     const uint32_t* __restrict__ nw, uint32_t* __restrict__ old, uint32_t* __restrict__ fr,
     int64_t W, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ mdeg,
-    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr) {
+    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, Counters* __restrict__ ctr,
+    BfsState::Published* pub, unsigned long long seq) {
   frontier_count_body<kDeg>(nw, old, fr, W, row_ptr, mdeg, blk_cnt, blk_deg, ctr);
+  publish_if_last(ctr, pub, seq);
 }
 
 __global__ void __launch_bounds__(kFrontierThreads) frontier_deg_kernel(
@@ -950,20 +991,6 @@ __global__ void __launch_bounds__(kFrontierThreads) frontier_write_kernel(
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
     int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
   frontier_write_body(fr, W, row_ptr, blk_cnt, blk_deg, queue, qdeg);
-}
-
-// End of a level: the counters go to host-mapped memory, then the level's
-// sequence number (after a system-wide fence, so the host that sees the
-// number sees the counters); the per-level sums are cleared for the next
-// level, which runs after this kernel in stream order.
-__global__ void publish_kernel(Counters* __restrict__ ctr, BfsState::Published* pub,
-                               unsigned long long seq) {
-  pub->c = *ctr;
-  ctr->nq = 0;
-  ctr->nq_edges = 0;
-  ctr->scanned = 0;
-  __threadfence_system();
-  *(volatile unsigned long long*)&pub->seq = seq;
 }
 
 __global__ void levels_kernel(const int64_t* __restrict__ pred, int64_t n,
@@ -1499,13 +1526,13 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
 
 }  // namespace
 
-// Publishes the level's counters and waits for them: polls the host-mapped
+// Waits for the level's counters: polls the host-mapped
 // sequence number, checking the stream every few thousand polls so that a
 // failed kernel ends the wait with its error instead of a hang.
 static Counters wait_level(BfsState& st, cudaStream_t s) {
+  // the level's last kernel publishes sequence number pub_seq + 1
   const unsigned long long seq = ++st.pub_seq;
-  publish_kernel<<<1, 1, 0, s>>>(st.ctr, st.dpub, seq);
-  check_cuda(cudaGetLastError(), "publish");
+  check_cuda(cudaGetLastError(), "level");
   volatile unsigned long long* flag = &st.hpub->seq;
   for (unsigned long long n = 1; *flag != seq; ++n) {
     if ((n & 4095) == 0) {
@@ -1606,7 +1633,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       launches += 2;
       frontier_count_kernel<false><<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(
           st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
-          st.ctr);
+          st.ctr, st.dpub, st.pub_seq + 1);
       frontier_in = qsize;
     } else {
       ++rs.num_bu_levels;
@@ -1614,11 +1641,12 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       const bool first = opt.bu_first && c.first;
       auto launch_wide = [&](auto kernel, int grid) {
         kernel<<<grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first,
-                                  c.first_inv, c.inv, pidx, out, level, st.ctr);
+                                  c.first_inv, c.inv, pidx, out, level, st.ctr, st.dpub,
+                                  st.pub_seq + 1);
       };
       auto launch_bu = [&](auto kernel) {
         kernel<<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.inv,
-                                     pidx, out, level, st.ctr);
+                                     pidx, out, level, st.ctr, st.dpub, st.pub_seq + 1);
       };
       if (opt.bu_kernel == 2)
         launch_wide(first ? bu_wide_kernel<2, 8, true> : bu_wide_kernel<2, 8, false>,
@@ -1638,7 +1666,6 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       cur ^= 1;
     }
     const Counters h = wait_level(st, s);
-    ++launches;
     global_nq_size = (int64_t)h.nq;
     if (forward) {
       global_nq_edges = (int64_t)h.nq_edges;
@@ -1699,7 +1726,7 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       if (!forward)  // after bottom-up: bits of vis[cur] not in vis[cur^1]
         frontier_count_kernel<true><<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(
             st.vis[cur], st.vis[cur ^ 1], st.fr, st.W, c.row_ptr, c.mdeg, st.blk_cnt, st.blk_deg,
-            st.ctr);
+            st.ctr, nullptr, 0);
       else  // after top-down: the counts are there, the degree sums not yet
         frontier_deg_kernel<<<(unsigned)st.nblk, kFrontierThreads, 0, s>>>(st.fr, st.W, c.row_ptr,
                                                                          st.blk_deg);

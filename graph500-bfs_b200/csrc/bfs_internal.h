@@ -13,7 +13,7 @@ struct Counters {
   unsigned long long qsize;     // length of the frontier queue
   unsigned long long qedges;    // CSR degree sum of the frontier queue
   int error;
-  int pad;
+  unsigned int blocks_done;     // blocks of the level's last kernel that finished
 };
 
 // Device-driven level loop of the single-source search (CUDA graph mode).
