@@ -155,7 +155,11 @@ def ncu_traffic(kernel):
         return None
 
 
-def dist_setup():
+def dist_setup(timeout_s=300):
+    """One process per GPU (torch.distributed.run sets RANK/WORLD_SIZE/...):
+    NCCL between the ranks' GPUs, gloo where CUDA is absent (host-side tests
+    of the replica plumbing). Only the timing bookkeeping crosses ranks: the
+    replicas share nothing else."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -166,30 +170,33 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return world, rank, local, dist
+
+
+def _reduce(dist, value, op):
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
 
 
 def barrier_max(dist, value):
     """Barrier, then the max of value over ranks."""
     if dist is None:
         return value
-    import torch
-
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _reduce(dist, value, dist.ReduceOp.MAX)
 
 
 def barrier_sum(dist, value):
     if dist is None:
         return value
-    import torch
-
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(dist, value, dist.ReduceOp.SUM)
 
 
 def build_flags(args):
