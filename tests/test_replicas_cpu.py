@@ -35,7 +35,8 @@ def test_two_ranks_max_time_sum_work():
 
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    # spawn throughout: no fork of a process that may hold threads
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
