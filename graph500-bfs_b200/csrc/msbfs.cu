@@ -50,6 +50,10 @@ __device__ __forceinline__ unsigned long long* plane_ptr(const BatchCtl* c, long
   return c->planes + L * c->R;
 }
 
+__device__ __forceinline__ uint32_t* rowbits_of(const BatchCtl* c, long long L) {
+  return c->rowbits + L * c->wstride;
+}
+
 // Zero-fills p[0, n) with 16-byte stores from thread t0 of a grid of
 // `stride` threads (p is 8-byte aligned: a plane starts at L * R words).
 __device__ __forceinline__ void zero_u64(unsigned long long* __restrict__ p, int64_t n,
@@ -63,20 +67,35 @@ __device__ __forceinline__ void zero_u64(unsigned long long* __restrict__ p, int
   if (((n - head) & 1) && t0 == 0) p[n - 1] = 0ull;
 }
 
-// Level start: clears the touched-row bitmap of the level and, when no
-// bottom-up sweep will write every row of the level's plane, zero-fills the
-// plane for the top-down push to OR into.
+// Level start of a level without a bottom-up sweep: zeroes the rows of the
+// level's plane that its bitmap marks (what an earlier batch left there) and
+// the bitmap, for the top-down push to OR into.  A bottom-up sweep does the
+// same for its own rows.  A marked word's 32 rows are zeroed whole, two rows
+// (16 bytes) per lane, 16 lanes per word; the loop is warp-uniform so the
+// lanes of a word have all read it before it is cleared.
 __global__ void batch_clear_kernel(const BatchCtl* __restrict__ ctl) {
+  if (ctl->has_bu) return;
   const long long L = ctl->level;
   const int64_t R = ctl->R;
-  const int64_t W = (R + 31) >> 5;
-  uint32_t* __restrict__ rb = ctl->rowbits[L & 1];
+  const int64_t npairs = ((R + 31) >> 5) * 16;
+  uint32_t* __restrict__ rb = rowbits_of(ctl, L);
   unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
-  const bool zero_plane = !ctl->has_bu;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int64_t i = t0; i < W; i += stride) rb[i] = 0u;
-  if (zero_plane) zero_u64(cur, R, t0, stride);
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = gw * 32; base < npairs; base += nwarps * 32) {
+    const int64_t q = base + lane;
+    const int64_t w = q >> 4;
+    const uint32_t bits = q < npairs ? rb[w] : 0u;
+    if (bits) {  // the whole 32-row block
+      // a marked word may cover rows past R (a pool marked whole)
+      const int64_t v = q * 2;
+      if (v < R) cur[v] = 0ull;
+      if (v + 1 < R) cur[v + 1] = 0ull;
+    }
+    __syncwarp();
+    if ((q & 15) == 0 && bits) rb[w] = 0u;
+  }
 }
 
 // Queue pass 1 (top-down levels): per-block count and degree sum of the rows
@@ -92,7 +111,7 @@ __global__ void __launch_bounds__(kQThreads) batch_queue_count_kernel(
   const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
-  const uint32_t* __restrict__ rb = ctl->rowbits[(L - 1) & 1];
+  const uint32_t* __restrict__ rb = rowbits_of(ctl, L - 1);
   const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
   int64_t cnt = 0, deg = 0;
   uint32_t bits = w < W ? rb[w] : 0u;
@@ -196,7 +215,7 @@ __global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
   const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
-  const uint32_t* __restrict__ rb = ctl->rowbits[(L - 1) & 1];
+  const uint32_t* __restrict__ rb = rowbits_of(ctl, L - 1);
   const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
   uint32_t take = 0;
   int64_t cnt = 0, deg = 0;
@@ -266,7 +285,7 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   unsigned long long* cur = plane_ptr(ctl, L);
   unsigned long long* seen = ctl->seen;
-  uint32_t* rb = ctl->rowbits[L & 1];
+  uint32_t* rb = rowbits_of(ctl, L);
   const int64_t total = qdeg[qsize];
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -299,7 +318,10 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
       if (m) {
         atomicOr(seen + u, m);
         atomicOr(cur + u, m);
-        atomicOr(rb + (u >> 5), 1u << (u & 31));
+        // the bitmap is L2-resident; most rows are marked by an earlier
+        // edge, and a read costs less than an atomic
+        const uint32_t bit = 1u << (u & 31);
+        if (!(__ldcg(rb + (u >> 5)) & bit)) atomicOr(rb + (u >> 5), bit);
         found |= m;
       }
     }
@@ -318,11 +340,14 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // own lane (kProbe 128 measured fastest).  Rows are sorted by
 // descending degree, so neighbour lists start with the hubs, which most
 // roots reach first.  The row's new bits are written to planes[L] and seen
-// by the lane that owns it, and every row of planes[L] is written (zero when
-// nothing is found), before the top-down push of the level ORs into it: no
-// atomics.  The frontier masks of level L-1 are
-// only read here, and a bit of U can only come from a neighbour at level
-// L-1 of that root, so the OR over neighbours is exact.
+// by the lane that owns it, before the top-down push of the level ORs into
+// planes[L]: no atomics.  A warp's 32 rows are one word of the plane's
+// bitmap of possibly non-zero rows; the warp writes its rows when it found
+// bits or the word marks some (left by an earlier batch), so the plane holds
+// exactly this level afterwards, and the word becomes the rows found.
+// The frontier masks of level L-1 are only read here, and a bit of U can
+// only come from a neighbour at level L-1 of that root, so the OR over
+// neighbours is exact.
 // first (may be null): the rows' first neighbours; an open row ORs its first
 // neighbour's mask (one coalesced read of first[] per warp) before loading
 // its row offsets, which it then needs only if that mask does not cover U.
@@ -339,20 +364,37 @@ __global__ void __launch_bounds__(256, 4) batch_bu_kernel(BatchCtl* __restrict__
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
   unsigned long long* __restrict__ seen = ctl->seen;
-  uint32_t* __restrict__ rb = ctl->rowbits[L & 1];
+  uint32_t* __restrict__ rb = rowbits_of(ctl, L);
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nchunks = (R + 31) >> 5;
   unsigned long long found = 0, scanned = 0, rows = 0;
+  // the seen masks and bitmap word of the warp's next chunk are loaded one
+  // chunk ahead (only this warp writes them), so a chunk without work costs
+  // no exposed load latency
+  unsigned long long s_next = ~0ull;
+  uint32_t d_next = 0;
+  if (gw < nchunks) {
+    const int64_t v0 = gw * 32 + lane;
+    s_next = v0 < R ? seen[v0] : ~0ull;
+    d_next = rb[gw];
+  }
   for (int64_t ch = gw; ch < nchunks; ch += nwarps) {
     const int64_t v = ch * 32 + lane;
     const bool valid = v < R;
-    const unsigned long long s = valid ? seen[v] : ~0ull;
+    const uint32_t dirty = d_next;
+    const unsigned long long s = s_next;
+    if (ch + nwarps < nchunks) {
+      const int64_t vn = v + nwarps * 32;
+      s_next = vn < R ? seen[vn] : ~0ull;
+      d_next = rb[ch + nwarps];
+    }
     const unsigned long long U = ~s & Bm;
     const unsigned work = __ballot_sync(kFull, U != 0);
     if (!work) {
-      if (valid) cur[v] = 0ull;
+      if (valid && dirty) cur[v] = 0ull;
+      if (lane == 0 && dirty) rb[ch] = 0u;
       continue;
     }
     rows += (lane == 0) ? __popc(work) : 0;
@@ -413,12 +455,11 @@ __global__ void __launch_bounds__(256, 4) batch_bu_kernel(BatchCtl* __restrict__
       }
     }
     const unsigned long long n = acc & U;
-    if (valid) {
-      cur[v] = n;
-      if (n) seen[v] = s | n;
-    }
     const unsigned hit = __ballot_sync(kFull, n != 0);
-    if (lane == 0 && hit) rb[ch] = hit;
+    // whole 256-byte blocks: partial sector writes cost DRAM reads
+    if (valid && (hit || dirty)) cur[v] = n;
+    if (valid && hit) seen[v] = s | n;
+    if (lane == 0 && (hit || dirty)) rb[ch] = hit;
     found |= n;
   }
   found = warp_or64(found);
@@ -534,7 +575,7 @@ __global__ void __launch_bounds__(kBatchMax) batch_control_kernel(
     if (r >= 0) {
       atomicOr(plane_ptr(ctl, L) + r, bit);
       atomicOr(c.seen + r, bit);
-      atomicOr(c.rowbits[L & 1] + (r >> 5), 1u << (r & 31));
+      atomicOr(rowbits_of(ctl, L) + (r >> 5), 1u << (r & 31));
       atomicOr(&s_seeded, bit);
     }
   }
@@ -609,7 +650,8 @@ __global__ void __launch_bounds__(kBatchMax) batch_control_kernel(
 struct BatchSetupArg {
   unsigned long long* planes;
   unsigned long long* seen;
-  uint32_t* rowbits[2];
+  uint32_t* rowbits;
+  long long wstride;
   long long R, capacity, nedges, nverts;
   double alpha, beta;
   int edgefactor, K;
@@ -617,28 +659,30 @@ struct BatchSetupArg {
   int lv[kBatchMax];       // its level
   // planes[0] is zero except at the rows the previous batch seeded there
   // (clear[0..nclear)); full_clear when that is not known (new pool, failed
-  // batch)
+  // batch), which also marks every row of the other planes as possibly
+  // non-zero
   int full_clear, nclear;
   int clear[kBatchMax];
 };
 
 // seen = 0, planes[0] = 0 and the touched-row bitmap of level 0 = 0.  Only
 // seeding writes planes[0], so after a batch it holds bits at that batch's
-// level-0 root rows alone, and clearing those rows restores it.
+// level-0 root rows alone, and clearing those rows restores it.  With
+// full_clear the bitmaps of planes 1 .. capacity-1 are set to all rows.
 __global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
   const int64_t n = a->R;
   unsigned long long* __restrict__ seen = a->seen;
   unsigned long long* __restrict__ p0 = a->planes;
-  uint32_t* __restrict__ rb = a->rowbits[0];
+  uint32_t* __restrict__ rb = a->rowbits;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool full = a->full_clear != 0;
   zero_u64(seen, n, t0, stride);
   if (full) zero_u64(p0, n, t0, stride);
   if (!full && t0 < a->nclear) p0[a->clear[t0]] = 0ull;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31) >> 5);
-       i += stride)
-    rb[i] = 0u;
+  for (int64_t i = t0; i < ((n + 31) >> 5); i += stride) rb[i] = 0u;
+  if (full)
+    for (int64_t i = a->wstride + t0; i < a->capacity * a->wstride; i += stride) rb[i] = ~0u;
 }
 
 // Initialises the control block for a new batch (64 threads).
@@ -658,8 +702,8 @@ __global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, const BatchSetupA
   if (t == 0) {
     ctl->planes = a.planes;
     ctl->seen = a.seen;
-    ctl->rowbits[0] = a.rowbits[0];
-    ctl->rowbits[1] = a.rowbits[1];
+    ctl->rowbits = a.rowbits;
+    ctl->wstride = a.wstride;
     ctl->R = a.R;
     ctl->capacity = a.capacity;
     ctl->nedges = a.nedges;
@@ -683,8 +727,10 @@ __global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, const BatchSetupA
 }
 
 // Points the control block at a larger plane pool and resumes the search.
-__global__ void batch_pool_kernel(BatchCtl* ctl, unsigned long long* planes, long long capacity) {
+__global__ void batch_pool_kernel(BatchCtl* ctl, unsigned long long* planes, uint32_t* rowbits,
+                                  long long capacity) {
   ctl->planes = planes;
+  ctl->rowbits = rowbits;
   ctl->capacity = capacity;
   ctl->done = 0;
 }
@@ -879,8 +925,7 @@ void BatchState::release(DeviceArena& arena) {
   d_arg = h_arg = nullptr;
   arena.free(planes);
   arena.free(seen);
-  arena.free(rowbits[0]);
-  arena.free(rowbits[1]);
+  arena.free(rowbits);
   arena.free(queue);
   arena.free(qdeg);
   queue = nullptr;
@@ -891,7 +936,7 @@ void BatchState::release(DeviceArena& arena) {
   cudaFreeHost(hctl);
   cudaFreeHost(hdone);
   planes = seen = nullptr;
-  rowbits[0] = rowbits[1] = nullptr;
+  rowbits = nullptr;
   blk_cnt = blk_deg = nullptr;
   ctl = nullptr;
   hctl = nullptr;
@@ -910,8 +955,7 @@ void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
   const int64_t W = (bs.R + 31) / 32;
   bs.nblk = (W + kQThreads - 1) / kQThreads;
   bs.seen = arena_alloc<unsigned long long>(arena, bs.R, "batch seen masks");
-  bs.rowbits[0] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
-  bs.rowbits[1] = arena_alloc<uint32_t>(arena, W + 1, "batch touched rows");
+  bs.wstride = (W + 4) & ~(int64_t)3;
   bs.queue = arena_alloc<int32_t>(arena, bs.R + 1, "batch frontier queue");
   bs.qdeg = arena_alloc<int64_t>(arena, bs.R + 2, "batch frontier degree prefix");
   bs.blk_cnt = arena_alloc<int64_t>(arena, bs.nblk + 1, "batch block counts");
@@ -925,11 +969,15 @@ void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
   // Level planes: 16 to start with (Kronecker searches need about 10),
   // fewer when memory is short; the search grows the pool when it runs out.
   for (int64_t cap = 16;; cap /= 2) {
+    unsigned long long* p = nullptr;
     try {
-      bs.planes = arena_alloc<unsigned long long>(arena, cap * bs.R, "batch level planes");
+      p = arena_alloc<unsigned long long>(arena, cap * bs.R, "batch level planes");
+      bs.rowbits = arena_alloc<uint32_t>(arena, cap * bs.wstride, "batch touched-row bitmaps");
+      bs.planes = p;
       bs.capacity = cap;
       break;
     } catch (const Error& e) {
+      arena.free(p);
       if (e.code != B200BFS_ERR_OOM || cap <= 2) throw;
     }
   }
@@ -939,12 +987,28 @@ void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
 void batch_grow(DeviceArena& arena, BatchState& bs, int64_t used, cudaStream_t s) {
   const int64_t cap = bs.capacity * 2;
   unsigned long long* np = arena_alloc<unsigned long long>(arena, cap * bs.R, "batch level planes");
+  uint32_t* nr = nullptr;
+  try {
+    nr = arena_alloc<uint32_t>(arena, cap * bs.wstride, "batch touched-row bitmaps");
+  } catch (...) {
+    arena.free(np);
+    throw;
+  }
   check_cuda(cudaMemcpyAsync(np, bs.planes, (size_t)used * bs.R * 8, cudaMemcpyDeviceToDevice, s),
              "copy planes");
-  batch_pool_kernel<<<1, 1, 0, s>>>(bs.ctl, np, cap);
+  // the bitmaps of the kept planes come along; the new planes are garbage,
+  // so every row of theirs is marked
+  check_cuda(cudaMemcpyAsync(nr, bs.rowbits, (size_t)used * bs.wstride * 4,
+                             cudaMemcpyDeviceToDevice, s),
+             "copy bitmaps");
+  check_cuda(cudaMemsetAsync(nr + used * bs.wstride, 0xFF, (size_t)(cap - used) * bs.wstride * 4, s),
+             "mark new planes");
+  batch_pool_kernel<<<1, 1, 0, s>>>(bs.ctl, np, nr, cap);
   check_cuda(cudaStreamSynchronize(s), "grow planes");
   arena.free(bs.planes);
+  arena.free(bs.rowbits);
   bs.planes = np;
+  bs.rowbits = nr;
   bs.capacity = cap;
 }
 
@@ -1097,8 +1161,8 @@ void run_batch(DeviceArena& arena, const Graph& g, BatchState& bs, cudaStream_t 
   }
   a.planes = bs.planes;
   a.seen = bs.seen;
-  a.rowbits[0] = bs.rowbits[0];
-  a.rowbits[1] = bs.rowbits[1];
+  a.rowbits = bs.rowbits;
+  a.wstride = bs.wstride;
   a.R = bs.R;
   a.capacity = bs.capacity;
   a.nedges = c.nedges;

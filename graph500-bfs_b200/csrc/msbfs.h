@@ -38,7 +38,12 @@ struct BatchCtl {
   // fixed during a search
   unsigned long long* planes;  // [capacity][R]: bit k of planes[L][v] <=> level_k(v) == L
   unsigned long long* seen;    // [R]: bits of the roots that reached v
-  uint32_t* rowbits[2];        // [R/32]: rows with a bit in planes[L], for L even / odd
+  // [capacity][wstride]: bitmap of the rows of planes[L] that may be
+  // non-zero (a superset of them), per plane.  A level clears only those rows
+  // of its plane, so a plane a batch leaves mostly zero costs the next batch
+  // little to reuse.
+  uint32_t* rowbits;
+  long long wstride;           // words per plane bitmap (>= (R + 31) / 32, multiple of 4)
   long long R;
   long long capacity;          // planes allocated
   long long nedges;            // num_global_edges (alpha test)
@@ -69,7 +74,8 @@ struct BatchState {
   int64_t nblk = 0;
   unsigned long long* planes = nullptr;
   unsigned long long* seen = nullptr;
-  uint32_t* rowbits[2] = {nullptr, nullptr};
+  uint32_t* rowbits = nullptr;  // [capacity][wstride], see BatchCtl
+  int64_t wstride = 0;
   int32_t* queue = nullptr;  // top-down queue rows
   int64_t* qdeg = nullptr;   // its degree prefix
   int64_t* blk_cnt = nullptr;
