@@ -70,31 +70,31 @@ __device__ __forceinline__ void zero_u64(unsigned long long* __restrict__ p, int
 // Level start of a level without a bottom-up sweep: zeroes the rows of the
 // level's plane that its bitmap marks (what an earlier batch left there) and
 // the bitmap, for the top-down push to OR into.  A bottom-up sweep does the
-// same for its own rows.  A marked word's 32 rows are zeroed whole, two rows
-// (16 bytes) per lane, 16 lanes per word; the loop is warp-uniform so the
-// lanes of a word have all read it before it is cleared.
+// same for its own rows.  Each lane reads one bitmap word (a warp reads 32
+// consecutive words); the warp then zeroes the 32-row block (256 bytes) of
+// each marked word together, one row per lane.
 __global__ void batch_clear_kernel(const BatchCtl* __restrict__ ctl) {
   if (ctl->has_bu) return;
   const long long L = ctl->level;
   const int64_t R = ctl->R;
-  const int64_t npairs = ((R + 31) >> 5) * 16;
+  const int64_t W = (R + 31) >> 5;
   uint32_t* __restrict__ rb = rowbits_of(ctl, L);
   unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = gw * 32; base < npairs; base += nwarps * 32) {
-    const int64_t q = base + lane;
-    const int64_t w = q >> 4;
-    const uint32_t bits = q < npairs ? rb[w] : 0u;
-    if (bits) {  // the whole 32-row block
+  for (int64_t base = gw * 32; base < W; base += nwarps * 32) {
+    const int64_t w = base + lane;
+    const uint32_t bits = w < W ? rb[w] : 0u;
+    unsigned marked = __ballot_sync(kFull, bits != 0);
+    if (bits) rb[w] = 0u;
+    while (marked) {
+      const int l = __ffs(marked) - 1;
+      marked &= marked - 1;
       // a marked word may cover rows past R (a pool marked whole)
-      const int64_t v = q * 2;
+      const int64_t v = (base + l) * 32 + lane;
       if (v < R) cur[v] = 0ull;
-      if (v + 1 < R) cur[v + 1] = 0ull;
     }
-    __syncwarp();
-    if ((q & 15) == 0 && bits) rb[w] = 0u;
   }
 }
 
@@ -102,46 +102,51 @@ __global__ void batch_clear_kernel(const BatchCtl* __restrict__ ctl) {
 // whose previous plane holds a top-down root.  Only rows marked in the
 // previous level's touched-row bitmap can, so the pass reads that bitmap
 // (one bit per row) and the plane entries of its set bits.  One thread per
-// bitmap word.
+// bitmap word; a tile of kQThreads words gives one partial, and a block
+// takes tiles blockIdx.x, blockIdx.x + gridDim.x, ... (a one-wave grid: the
+// kernel runs at every level and returns at once on bottom-up-only ones).
 __global__ void __launch_bounds__(kQThreads) batch_queue_count_kernel(
     const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
-    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg) {
+    int64_t* __restrict__ blk_cnt, int64_t* __restrict__ blk_deg, int64_t ntiles) {
   if (!ctl->has_td) return;
   const long long L = ctl->level;
   const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   const uint32_t* __restrict__ rb = rowbits_of(ctl, L - 1);
-  const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
-  int64_t cnt = 0, deg = 0;
-  uint32_t bits = w < W ? rb[w] : 0u;
-  while (bits) {
-    const int64_t v = w * 32 + __ffs(bits) - 1;
-    bits &= bits - 1;
-    if (prev[v] & T) {
-      ++cnt;
-      deg += row_ptr[v + 1] - row_ptr[v];
-    }
-  }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    cnt += __shfl_xor_sync(kFull, cnt, o);
-    deg += __shfl_xor_sync(kFull, deg, o);
-  }
   __shared__ int64_t s_c[kQThreads / 32], s_d[kQThreads / 32];
-  if (lane_id() == 0) {
-    s_c[threadIdx.x >> 5] = cnt;
-    s_d[threadIdx.x >> 5] = deg;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int64_t a = 0, b = 0;
-    for (int i = 0; i < kQThreads / 32; ++i) {
-      a += s_c[i];
-      b += s_d[i];
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t w = tile * kQThreads + threadIdx.x;
+    int64_t cnt = 0, deg = 0;
+    uint32_t bits = w < W ? rb[w] : 0u;
+    while (bits) {
+      const int64_t v = w * 32 + __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (prev[v] & T) {
+        ++cnt;
+        deg += row_ptr[v + 1] - row_ptr[v];
+      }
     }
-    blk_cnt[blockIdx.x] = a;
-    blk_deg[blockIdx.x] = b;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      cnt += __shfl_xor_sync(kFull, cnt, o);
+      deg += __shfl_xor_sync(kFull, deg, o);
+    }
+    if (lane_id() == 0) {
+      s_c[threadIdx.x >> 5] = cnt;
+      s_d[threadIdx.x >> 5] = deg;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t a = 0, b = 0;
+      for (int i = 0; i < kQThreads / 32; ++i) {
+        a += s_c[i];
+        b += s_d[i];
+      }
+      blk_cnt[tile] = a;
+      blk_deg[tile] = b;
+    }
+    __syncthreads();
   }
 }
 
@@ -205,63 +210,67 @@ __global__ void __launch_bounds__(1024) batch_queue_scan_kernel(BatchCtl* __rest
   }
 }
 
-// Queue pass 3: queue rows (in row order) and their degree prefix.
+// Queue pass 3: queue rows (in row order) and their degree prefix; tiles as
+// in pass 1.
 __global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
     const BatchCtl* __restrict__ ctl, const int64_t* __restrict__ row_ptr,
     const int64_t* __restrict__ blk_cnt, const int64_t* __restrict__ blk_deg,
-    int32_t* __restrict__ queue, int64_t* __restrict__ qdeg) {
+    int32_t* __restrict__ queue, int64_t* __restrict__ qdeg, int64_t ntiles) {
   if (!ctl->has_td) return;
   const long long L = ctl->level;
   const int64_t W = (ctl->R + 31) >> 5;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
   const uint32_t* __restrict__ rb = rowbits_of(ctl, L - 1);
-  const int64_t w = (int64_t)blockIdx.x * kQThreads + threadIdx.x;
-  uint32_t take = 0;
-  int64_t cnt = 0, deg = 0;
-  {
-    uint32_t bits = w < W ? rb[w] : 0u;
-    while (bits) {
-      const int b = __ffs(bits) - 1;
-      bits &= bits - 1;
-      const int64_t v = w * 32 + b;
-      if (prev[v] & T) {
-        take |= 1u << b;
-        ++cnt;
-        deg += row_ptr[v + 1] - row_ptr[v];
-      }
-    }
-  }
-  int64_t ic = cnt, id = deg;
-  warp_scan2(ic, id);
   __shared__ int64_t s_c[kQThreads / 32], s_d[kQThreads / 32];
   const int wid = threadIdx.x >> 5;
-  if (lane_id() == 31) {
-    s_c[wid] = ic;
-    s_d[wid] = id;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int64_t a = 0, b = 0;
-    for (int i = 0; i < kQThreads / 32; ++i) {
-      const int64_t xa = s_c[i], xb = s_d[i];
-      s_c[i] = a;
-      s_d[i] = b;
-      a += xa;
-      b += xb;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t w = tile * kQThreads + threadIdx.x;
+    uint32_t take = 0;
+    int64_t cnt = 0, deg = 0;
+    {
+      uint32_t bits = w < W ? rb[w] : 0u;
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int64_t v = w * 32 + b;
+        if (prev[v] & T) {
+          take |= 1u << b;
+          ++cnt;
+          deg += row_ptr[v + 1] - row_ptr[v];
+        }
+      }
     }
-  }
-  __syncthreads();
-  int64_t pos = blk_cnt[blockIdx.x] + s_c[wid] + ic - cnt;
-  int64_t dpos = blk_deg[blockIdx.x] + s_d[wid] + id - deg;
-  while (take) {
-    const int64_t v = w * 32 + __ffs(take) - 1;
-    take &= take - 1;
-    const int64_t d = row_ptr[v + 1] - row_ptr[v];
-    queue[pos] = (int32_t)v;
-    qdeg[pos] = dpos;
-    ++pos;
-    dpos += d;
+    int64_t ic = cnt, id = deg;
+    warp_scan2(ic, id);
+    if (lane_id() == 31) {
+      s_c[wid] = ic;
+      s_d[wid] = id;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t a = 0, b = 0;
+      for (int i = 0; i < kQThreads / 32; ++i) {
+        const int64_t xa = s_c[i], xb = s_d[i];
+        s_c[i] = a;
+        s_d[i] = b;
+        a += xa;
+        b += xb;
+      }
+    }
+    __syncthreads();
+    int64_t pos = blk_cnt[tile] + s_c[wid] + ic - cnt;
+    int64_t dpos = blk_deg[tile] + s_d[wid] + id - deg;
+    while (take) {
+      const int64_t v = w * 32 + __ffs(take) - 1;
+      take &= take - 1;
+      const int64_t d = row_ptr[v + 1] - row_ptr[v];
+      queue[pos] = (int32_t)v;
+      qdeg[pos] = dpos;
+      ++pos;
+      dpos += d;
+    }
+    __syncthreads();
   }
 }
 
@@ -351,9 +360,12 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
 // first (may be null): the rows' first neighbours; an open row ORs its first
 // neighbour's mask (one coalesced read of first[] per warp) before loading
 // its row offsets, which it then needs only if that mask does not cover U.
-// Launched with 4 blocks per SM, all resident (at most 64 registers).
+// Launched with 5 blocks per SM, all resident (at most 51 registers): the
+// sweep is bound by load latency on the sparser levels, and 5 blocks measured
+// faster than 4 (SCALE 28 64-root batch 22.4 against 22.7 ms) and 6 (23.4 ms,
+// with spills at 40 registers).
 template <int kProbe, int kPer>
-__global__ void __launch_bounds__(256, 4) batch_bu_kernel(BatchCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(256, 5) batch_bu_kernel(BatchCtl* __restrict__ ctl,
                                                        const int64_t* __restrict__ row_ptr,
                                                        const int32_t* __restrict__ col,
                                                        const int32_t* __restrict__ first) {
@@ -1023,13 +1035,18 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
                   cudaGraphConditionalHandle cond, int use_cond, const cudaEvent_t* ev) {
   const Csr& c = batch_csr(g);
   const int B = 256;
-  const unsigned nblk = (unsigned)std::max<int64_t>(bs.nblk, 1);
+  const int64_t ntiles = std::max<int64_t>(bs.nblk, 1);
+  const unsigned qc_grid = (unsigned)std::min<int64_t>(
+      ntiles, (int64_t)sms * blocks_per_sm(batch_queue_count_kernel, kQThreads));
+  const unsigned qw_grid = (unsigned)std::min<int64_t>(
+      ntiles, (int64_t)sms * blocks_per_sm(batch_queue_write_kernel, kQThreads));
   if (ev) check_cuda(cudaEventRecord(ev[0], s), "event");
   batch_clear_kernel<<<grid_for(bs.R, B, sms, 8), B, 0, s>>>(bs.ctl);
-  batch_queue_count_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg);
+  batch_queue_count_kernel<<<qc_grid, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
+                                                        ntiles);
   batch_queue_scan_kernel<<<1, 1024, 0, s>>>(bs.ctl, bs.blk_cnt, bs.blk_deg, bs.nblk, bs.qdeg);
-  batch_queue_write_kernel<<<nblk, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt, bs.blk_deg,
-                                                      bs.queue, bs.qdeg);
+  batch_queue_write_kernel<<<qw_grid, kQThreads, 0, s>>>(bs.ctl, c.row_ptr, bs.blk_cnt,
+                                                        bs.blk_deg, bs.queue, bs.qdeg, ntiles);
   if (ev) check_cuda(cudaEventRecord(ev[1], s), "event");
   auto bu = batch_bu_kernel<128, 4>;
   switch (bs.bu_probe * 16 + bs.bu_round) {
@@ -1047,7 +1064,7 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
     case 128 * 16 + 8: bu = batch_bu_kernel<128, 8>; break;
     default: break;
   }
-  bu<<<sms * 4, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
+  bu<<<sms * 5, B, 0, s>>>(bs.ctl, c.row_ptr, c.col, c.first);
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
   batch_td_kernel<<<sms * blocks_per_sm(batch_td_kernel, B), B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg,
                                                                       c.row_ptr, c.col);
@@ -1082,6 +1099,8 @@ void build_graph(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
   // occupancy queries stay outside the capture
   blocks_per_sm(batch_td_kernel, 256);
   blocks_per_sm(batch_stats_kernel, 256);
+  blocks_per_sm(batch_queue_count_kernel, kQThreads);
+  blocks_per_sm(batch_queue_write_kernel, kQThreads);
   check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
   cudaGraph_t cg = nullptr;
   cudaGraph_t body = nullptr;
