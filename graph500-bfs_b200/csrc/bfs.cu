@@ -146,9 +146,15 @@ __device__ __forceinline__ int64_t assembled_entry(int32_t m, int64_t u,
 
 // Four ids per thread: one 16-byte map load, two 16-byte pred stores
 // (pred and pmap are 256-byte aligned; n4 = n / 4, the tail done by thread 0).
+// sparse: pred already holds the entries of every vertex outside the
+// searched rows (-1, or its tree parent at level 0xFFFF), except at
+// prev_root (and the previous CoreBFS climb, which the caller restores), so
+// a group of four such vertices is not written: a third of the ids are rows
+// at SCALE 28, and one group in five has none.
 __device__ __forceinline__ void assemble_body(const int32_t* __restrict__ pmap, int64_t n,
                                               const uint32_t* __restrict__ vis,
                                               const int64_t* __restrict__ rp, int64_t root,
+                                              int64_t prev_root, int sparse,
                                               int64_t* __restrict__ pred) {
   const int64_t n4 = n >> 2;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,6 +164,9 @@ __device__ __forceinline__ void assemble_body(const int32_t* __restrict__ pmap, 
   for (int64_t i = t0; i < n4; i += stride) {
     const int4 m = __ldg(m4 + i);
     const int64_t u = 4 * i;
+    if (sparse && (m.x & m.y & m.z & m.w) < 0 && (uint64_t)(root - u) >= 4 &&
+        (uint64_t)(prev_root - u) >= 4)
+      continue;
     p2[2 * i] = make_longlong2(assembled_entry(m.x, u, vis, rp, root),
                                assembled_entry(m.y, u + 1, vis, rp, root));
     p2[2 * i + 1] = make_longlong2(assembled_entry(m.z, u + 2, vis, rp, root),
@@ -170,8 +179,23 @@ __device__ __forceinline__ void assemble_body(const int32_t* __restrict__ pmap, 
 __global__ void assemble_pred_kernel(const int32_t* __restrict__ pmap, int64_t n,
                                      const uint32_t* __restrict__ vis,
                                      const int64_t* __restrict__ rp, int64_t root,
+                                     int64_t prev_root, int sparse,
                                      int64_t* __restrict__ pred) {
-  assemble_body(pmap, n, vis, rp, root, pred);
+  assemble_body(pmap, n, vis, rp, root, prev_root, sparse, pred);
+}
+
+// Number of 4-id groups of pmap (n4 of them) holding a searched row.
+__global__ void core_groups_kernel(const int32_t* __restrict__ pmap, int64_t n4,
+                                   unsigned long long* __restrict__ count) {
+  const int4* m4 = reinterpret_cast<const int4*>(pmap);
+  unsigned long long c = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int4 m = __ldg(m4 + i);
+    c += (m.x & m.y & m.z & m.w) >= 0;  // not all four negative
+  }
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+  if (lane_id() == 0 && c) atomicAdd(count, c);
 }
 
 // pmap from the row map and the CoreBFS tree parents (tp null without CoreBFS).
@@ -1066,7 +1090,8 @@ __global__ void sg_assemble_kernel(const SingleCtl* __restrict__ c, const SgArg*
                                    uint32_t* const* __restrict__ vis_pp,
                                    const int32_t* __restrict__ pmap, int64_t n,
                                    const int64_t* __restrict__ rp, int64_t* __restrict__ pred) {
-  assemble_body(pmap, n, vis_pp[c->cur], rp, a->root, pred);
+  assemble_body(pmap, n, vis_pp[c->cur], rp, a->root, a->sparse ? a->prev_root : -1, a->sparse,
+                pred);
 }
 
 // Level start (host loop: ++level, at[8], prev_nq, forward, clear counters).
@@ -1254,8 +1279,10 @@ __global__ void sg_control_kernel(SingleCtl* __restrict__ c, const SgArg* __rest
 
 // Algorithmic bytes of the assembly pass: the map and pred over every id,
 // the rp entries of the reached rows, the visited bitmap.
-int64_t assembly_bytes(const BfsState& st, int64_t visited) {
-  return 12 * st.pred_size + 8 * visited + 4 * st.W;
+int64_t assembly_bytes(const BfsState& st, int64_t visited, bool sparse) {
+  // map read + pred writes + row-order entries of the reached rows + bitmap
+  const int64_t written = sparse ? 4 * st.core_groups : st.pred_size;
+  return 4 * st.pred_size + 8 * written + 8 * visited + 4 * st.W;
 }
 
 void build_pred_assembly(DeviceArena& arena, const Graph& g, BfsState& st, cudaStream_t s,
@@ -1265,8 +1292,16 @@ void build_pred_assembly(DeviceArena& arena, const Graph& g, BfsState& st, cudaS
   pred_map_kernel<<<grid_for(st.pred_size, 256, sms, 8), 256, 0, s>>>(
       g.csr.rank, g.core.enabled ? g.core.tree_parent : nullptr, g.nverts, st.pred_size,
       st.pmap);
+  // the groups a sparse assembly writes (scratch: the block counts)
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(st.blk_cnt);
+  check_cuda(cudaMemsetAsync(cnt, 0, sizeof(*cnt), s), "memset");
+  core_groups_kernel<<<grid_for(st.pred_size / 4, 256, sms, 8), 256, 0, s>>>(
+      st.pmap, st.pred_size / 4, cnt);
+  unsigned long long h = 0;
+  check_cuda(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaGetLastError(), "pred assembly map");
   check_cuda(cudaStreamSynchronize(s), "pred assembly map");
+  st.core_groups = (int64_t)h;
 }
 
 void BfsState::allocate(DeviceArena& arena, const Graph& g) {
@@ -1485,6 +1520,10 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   a.beta = beta;
   a.edgefactor = edgefactor;
   a.want_at = at != nullptr;
+  // as in the host loop: sparse when the last writer of pred was an
+  // assembled search
+  const bool sparse = assemble && st.assembled && st.pred_clean;
+  a.sparse = sparse ? 1 : 0;
   for (int i = 0; i < 9; ++i) a.at[i] = at ? at[i] : -1;
   check_cuda(cudaMemcpyAsync(st.sarg, st.hsarg, sizeof(SgArg), cudaMemcpyHostToDevice, s),
              "search arguments");
@@ -1496,6 +1535,7 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   if (c.done == 3) throw Error{B200BFS_ERR_OVERFLOW, "more than 0xFFFE BFS levels"};
   st.pred_clean = true;
   st.prev_root = root;
+  st.asm_sparse = sparse;
   st.assembled = assemble;
   if (at)
     for (int i = 0; i < 9; ++i) at[i] = c.at[i];
@@ -1518,7 +1558,8 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
     rs.bu_bytes = c.bu_bytes;
     rs.algorithmic_bytes =
         c.bytes + 4 * st.W +
-        (assemble ? assembly_bytes(st, c.visited) : 8 * std::max<int64_t>(st.R - c.visited, 0));
+        (assemble ? assembly_bytes(st, c.visited, sparse)
+                  : 8 * std::max<int64_t>(st.R - c.visited, 0));
     rs.kernel_launches = 3 + kSgLevelLaunches * (int)(c.num_td + c.num_bu);
     *stats = rs;
   }
@@ -1737,13 +1778,18 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       qsize = global_nq_size;
     }
   }
+  // the last writer of pred was an assembled search: every entry outside
+  // the searched rows already holds its value
+  const bool sparse = assemble && st.assembled && st.pred_clean;
+  st.asm_sparse = sparse;
   if (assemble) {
     check_cuda(cudaEventRecord(st.event(nev), s), "event");
     assemble_pred_kernel<<<grid_for(st.pred_size / 4, B, sms, 8), B, 0, s>>>(
-        st.pmap, st.pred_size, st.vis[cur], st.rp, root, st.pred);
+        st.pmap, st.pred_size, st.vis[cur], st.rp, root, sparse ? st.prev_root : -1,
+        sparse ? 1 : 0, st.pred);
     check_cuda(cudaEventRecord(st.event(nev + 1), s), "event");
     nev += 2;
-    rs.pred_bytes = assembly_bytes(st, visited);
+    rs.pred_bytes = assembly_bytes(st, visited, sparse);
     bytes += rs.pred_bytes;
   } else {
     reset_unvisited_kernel<<<grid_for(st.W, B, sms, 8), B, 0, s>>>(st.vis[cur], st.W, c.inv,

@@ -27,6 +27,7 @@ struct SgArg {
   long long root, prev_root, root_level;
   double alpha, beta;
   int edgefactor, want_at;
+  int sparse, pad;  // sparse pred assembly (see BfsState::asm_sparse)
   long long at[9];
 };
 // Control block: the state the host loop keeps in local variables.
@@ -82,6 +83,10 @@ struct BfsState {
   int64_t* rp = nullptr;                  // [R] row-order pred entries
   int32_t* pmap = nullptr;                // [pred_size]
   bool assembled = false;                 // the last search used the assembly
+  // and wrote only the 4-id groups holding a searched row (the others kept
+  // their entries from the search before); core_groups counts those groups
+  bool asm_sparse = false;
+  int64_t core_groups = 0;
   // device-driven level loop (graph mode)
   SingleCtl* sctl = nullptr;
   SingleCtl* hsctl = nullptr;             // pinned mirror
@@ -137,7 +142,7 @@ inline bool use_pred_assembly(const Graph&, const RunOptions& o) { return o.pred
 // and tree parents; synchronises the stream.
 void build_pred_assembly(DeviceArena& arena, const Graph& g, BfsState& st, cudaStream_t s,
                          int sms);
-int64_t assembly_bytes(const BfsState& st, int64_t visited);
+int64_t assembly_bytes(const BfsState& st, int64_t visited, bool sparse);
 // After the search's stream work is complete: the assembly pass time.
 void finish_run_stats(BfsState& st, b200bfs_run_stats* stats);
 

@@ -490,7 +490,7 @@ void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   run_bfs_core(g, st, s, sms, u, lv, edgefactor, alpha, beta, at, opt, stats);
   int launches;
   int64_t bytes;
-  if (st.assembled) {
+  if (st.assembled && !st.asm_sparse) {
     // the assembly pass wrote every tree parent with level 0xFFFF: only this
     // climb differs
     RewriteArg a;
@@ -504,14 +504,15 @@ void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     launches = 1;
     bytes = 16 * a.n;
     st.tree_clean = true;
-  } else if (!st.tree_clean) {
+  } else if (!st.assembled && !st.tree_clean) {
     // write_tree_parents (corebfs_adaptor.hpp:285-301): every pruned vertex
     launches = core_write_tree(g, st.pred, pv, pe, s, sms);
     bytes = 16 * g.core.tree_vertices;
     st.tree_clean = true;
   } else {
     // pred already holds every tree parent with level 0xFFFF except on the
-    // previous climb: put those back (unless on this climb), then this climb
+    // previous climb (a sparse assembly left the tree parents as they were):
+    // put those back (unless on this climb), then this climb
     RewriteArg a;
     a.n = 0;
     const std::vector<int32_t>& tp = g.core.h_tree_parent;
@@ -531,6 +532,7 @@ void core_run_bfs(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     check_cuda(cudaGetLastError(), "core climb");
     launches = 1;
     bytes = 16 * a.n;
+    st.tree_clean = true;
   }
   st.prev_path_v = pv;
   if (stats) {
