@@ -1506,6 +1506,7 @@ void run_bfs_core_graph(const Graph& g, BfsState& st, cudaStream_t s, int sms, i
   if (!st.sgexec ||
       st.skey != sg_key(g, st, sms, opt.td_kernel, opt.force_direction, bu_first, assemble))
     sg_build_graph(g, st, s, sms, opt.td_kernel, opt.force_direction, bu_first, assemble);
+  if (!assemble) st.assembled = false;  // as in run_bfs_core
   if (!st.pred_clean && !assemble) {
     st.tree_clean = false;
     init_kernel<<<grid_for(st.pred_size / 2, 256, sms, 8), 256, 0, s>>>(
@@ -1615,6 +1616,9 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
   if (assemble && !st.pmap) throw Error{B200BFS_ERR_STATE, "pred assembly map not built"};
   const int32_t* pidx = assemble ? nullptr : c.inv;
   int64_t* out = assemble ? st.rp : st.pred;
+  // a direct search writes pred as it goes: from here on, even if it fails,
+  // the next assembly must write every group
+  if (!assemble) st.assembled = false;
   const bool fill_pred = !st.pred_clean && !assemble;
   if (fill_pred) st.tree_clean = false;
   init_kernel<<<grid_for(std::max(fill_pred ? st.pred_size / 2 : 0, st.W), B, sms, 8), B, 0, s>>>(
