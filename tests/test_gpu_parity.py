@@ -227,6 +227,48 @@ def test_corebfs_parity(engine, oracle_graphs, scale, assemble):
     engine.end()
 
 
+def test_sparse_assembly_restores_climbs(engine, oracle_graphs):
+    """After a search that used the assembly pass, the next pass writes only
+    the groups of four ids that hold a searched row; the previous root's
+    entry and the previous CoreBFS climb must go back to their values.
+    Roots at the ends of the deepest climbs, alternating with core roots
+    and with each other, leave tree entries and levels equal to the oracle's
+    after every search."""
+    import b200bfs
+
+    scale = 14
+    edges, g = oracle_graphs(scale)
+    core = O.Core(g)
+    engine.generate_graph(scale, 16, flags=b200bfs.BUILD_COREBFS)
+    engine.prepare(16)
+    engine.set_option("pred_assemble", 1)
+    tp = core.tree_parent
+    depth = np.zeros(g.nverts, dtype=np.int64)
+    for v in np.nonzero(tp >= 0)[0]:
+        d, u = 0, int(v)
+        while tp[u] >= 0:
+            u = int(tp[u])
+            d += 1
+        depth[v] = d
+    deep = [int(v) for v in np.argsort(-depth, kind="stable")[:3] if depth[v] > 0]
+    assert len(deep) == 3 and depth[deep[0]] >= 2
+    he = core.has_edge()
+    core_roots = [int(r) for r in O.find_roots(he, 1 << scale, 8) if tp[int(r)] < 0][:2]
+    assert len(core_roots) == 2
+    seq = [deep[0], core_roots[0], deep[1], deep[2], deep[0], core_roots[1], deep[1]]
+    for r in seq:
+        engine.run(r, 16)
+        pred = engine.get_pred()[: g.nverts]
+        ref_pred, _, _ = core.bfs(r)
+        tree = O.pred_levels(ref_pred) == 0xFFFF
+        assert np.array_equal(pred[tree], ref_pred[tree]), r
+        assert np.array_equal(O.pred_levels(pred), O.pred_levels(ref_pred)), r
+        err, cnt = O.validate(edges, 1 << scale, pred, r, corebfs=True)
+        assert err == 0, r
+        assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(r)), r
+    engine.end()
+
+
 def test_errors_are_status_codes(engine):
     import b200bfs
 
