@@ -286,7 +286,9 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * dense per-row array first, the default), "td_unroll" (1, 2 or 4: 32-entry
  * steps a lane of top-down form 5 handles together), "pred_assemble" (1:
  * the levels write a row-order buffer and one pass over the original ids
- * writes pred, the default; 0: the levels write pred by original id),
+ * writes pred, the default; after a search of this kind the pass leaves out
+ * the ids whose entries cannot change (no edge, or a CoreBFS tree vertex off
+ * both climbs); 0: the levels write pred by original id),
  * "force_direction" (0 = alpha/beta rule, 1 = top-down only, 2 = bottom-up
  * from level 2),
  * "single_graph" (1: b200bfs_run runs its level loop as a CUDA graph on the
