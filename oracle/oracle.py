@@ -242,3 +242,40 @@ def pred_levels(pred):
 def pred_parents(pred):
     pred = np.asarray(pred, dtype=np.int64)
     return (pred << 16) >> 16
+
+
+def resolve_levels(pred):
+    """Exact per-vertex levels of a pred in the reference encoding, with
+    CoreBFS tree entries (level field 0xFFFF, corebfs_adaptor.hpp:290-296)
+    given their parent's level + 1, resolved round by round as
+    validate.hpp:1040-1141 does; -1 unreached.  Returns (levels, tree) with
+    tree[v] the parent of a tree entry, -1 elsewhere."""
+    pred = np.asarray(pred, dtype=np.int64)
+    reached = pred != -1
+    lv = np.where(reached, (pred >> 48) & 0xFFFF, -1).astype(np.int64)
+    par = np.where(reached, pred & ((1 << 48) - 1), -1).astype(np.int64)
+    tree = np.where(lv == 0xFFFF, par, -1)
+    while True:
+        todo = np.nonzero(lv == 0xFFFF)[0]
+        if todo.size == 0:
+            break
+        pl = lv[par[todo]]
+        ok = (pl != 0xFFFF) & (pl >= 0)
+        if not ok.any():
+            raise ValueError("tree entries whose parents never resolve")
+        lv[todo[ok]] = pl[ok] + 1
+    return lv, tree
+
+
+def find_roots_in_large_graph(has_edge, nglobalverts, num_roots, search_levels, seed=0):
+    """main.cc:334-359: roots from find_roots(seed, 0); while any root's search
+    has at most REMOVE_ROOTS_LEVEL_THED = 3 levels (auto_tuning_data[8]) and
+    SCALE > REMOVE_ROOTS_SCALE_THED = 6, pick again with the next seed.
+    search_levels(root) returns that root's auto_tuning_data[8]."""
+    r = seed
+    scale = int(nglobalverts).bit_length() - 1
+    while True:
+        roots = find_roots(has_edge, nglobalverts, num_roots, r, 0)
+        r += 1
+        if scale <= 6 or all(search_levels(int(x)) > 3 for x in roots):
+            return roots
