@@ -39,7 +39,7 @@ SYMBOLS = [
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
-    "b200bfs_validate", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
+    "b200bfs_validate", "b200bfs_validate_pred", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
     "b200bfs_server_start", "b200bfs_server_add_graph", "b200bfs_server_graph_info",
     "b200bfs_server_find_roots", "b200bfs_tune_engine",
     "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
@@ -184,6 +184,8 @@ def load_library(path=LIB_PATH):
     L.b200bfs_get_level_stats.argtypes = [H, vp, i32, P(ctypes.c_int)]
     L.b200bfs_end.argtypes = [H]
     L.b200bfs_validate.argtypes = [H, i64, P(ctypes.c_int64), P(ctypes.c_int64)]
+    L.b200bfs_validate_pred.argtypes = [H, i64, ctypes.c_void_p, ctypes.c_int,
+                                        P(ctypes.c_int64), P(ctypes.c_int64)]
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
     L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
     L.b200bfs_tune_engine.argtypes = [H, vp, i32, i32, dbl, dbl, i32, P(TuneReport)]
@@ -377,6 +379,22 @@ class Engine:
         cnt = ctypes.c_int64()
         self.check(self.L.b200bfs_validate(self.h, int(root), ctypes.byref(err),
                                            ctypes.byref(cnt)))
+        return err.value, cnt.value
+
+    def validate_pred(self, root, pred, corebfs=None):
+        """Graph500 validation of a caller's pred (host array of pred_size
+        int64 entries) on the device (validate_bfs_result, validate.hpp:1269);
+        corebfs defaults to the graph's mode.  Returns (errors, edges)."""
+        pred = np.ascontiguousarray(pred, dtype=np.int64)
+        if pred.size != self.info().pred_size:
+            raise ValueError("pred must have pred_size entries")
+        if corebfs is None:
+            corebfs = bool(self.info().corebfs)
+        err = ctypes.c_int64()
+        cnt = ctypes.c_int64()
+        self.check(self.L.b200bfs_validate_pred(self.h, int(root), pred.ctypes.data,
+                                                1 if corebfs else 0, ctypes.byref(err),
+                                                ctypes.byref(cnt)))
         return err.value, cnt.value
 
 

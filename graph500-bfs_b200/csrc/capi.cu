@@ -639,7 +639,18 @@ int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors, int64_t* 
   return guarded(h, [&](Engine& e) {
     require(errors && edge_visit_count, B200BFS_ERR_INVALID, "null output");
     require(e.have_run, B200BFS_ERR_STATE, "no search has run");
-    b200bfs::validate_device(e.arena, e.stream, e.sms, e.g, e.st, root, errors, edge_visit_count);
+    b200bfs::validate_device(e.arena, e.stream, e.sms, e.g, e.st.pred, e.g.core.enabled, root,
+                             errors, edge_visit_count);
+  });
+}
+
+int b200bfs_validate_pred(b200bfs_handle* h, int64_t root, const int64_t* pred, int corebfs,
+                          int64_t* errors, int64_t* edge_visit_count) {
+  return guarded(h, [&](Engine& e) {
+    require(pred && errors && edge_visit_count, B200BFS_ERR_INVALID, "null argument");
+    require(e.g.built, B200BFS_ERR_STATE, "no graph");
+    b200bfs::validate_device(e.arena, e.stream, e.sms, e.g, pred, corebfs != 0, root, errors,
+                             edge_visit_count);
   });
 }
 

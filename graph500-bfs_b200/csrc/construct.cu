@@ -223,7 +223,10 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
   g.nverts = int64_t(1) << est;
   g.pred_size = std::max<int64_t>(g.nverts, int64_t(1) << 16);
   g.group_reorder = group_reorder;
-  const int group_bits = group_reorder ? std::min(16, est) : 0;
+  // Group width of the group order: min(16, 48 - local id bits)
+  // (graph_constructor.hpp:704-712), which is 16 for every SCALE <= 30 here.
+  // Below SCALE 16 one group holds every id, as with a narrower group.
+  const int group_bits = group_reorder ? 16 : 0;
   g.reorder_bits = group_bits;
   const int64_t n = g.nverts;
 

@@ -1,20 +1,24 @@
 // BFS entry point that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is
-// being captured, allocators that own all of device memory (a caching pool
-// that must not be bypassed), or hosts that hand over a fixed memory budget
-// and forbid further allocation.  b200bfs_bfs_noalloc serves them: the caller
-// passes a CSR and the output array already on the device, and the search
-// keeps its two visited bitmaps and its counter in one file-scope device
-// array of fixed size (B200BFS_NOALLOC_MAX_ROWS vertices, 4 MiB of bitmaps),
-// which every GPU that loads the library holds until the process exits.
+// Some callers cannot call cudaMalloc: applications whose caching allocator
+// owns the device memory (a framework's memory pool that must not be
+// bypassed, or that has already reserved nearly all of the GPU), and hosts
+// that give a library a fixed device-memory budget at start-up and forbid
+// allocations after it.  b200bfs_bfs_noalloc serves them: the caller passes a
+// CSR and the output array already on the device, and the search keeps its
+// two visited bitmaps and its counter in one file-scope device array of fixed
+// size (B200BFS_NOALLOC_MAX_ROWS vertices, 4 MiB of bitmaps), which every GPU
+// that loads the library holds until the process exits.
 //
 // It is the bottom-up step of the engine (bfs.cu, bu_kernel) in a variant
 // over caller row ids: every level, each warp owns 32 vertices, each
 // unvisited vertex looks for a neighbour visited before the level, and the
 // next bitmap word is built with __ballot_sync.  Bottom-up from the first
-// level is still a correct BFS (the first level finds the root's
-// neighbours), so no frontier queue -- and no more scratch -- is needed.
+// level is still a correct BFS on a symmetric CSR (the first level finds the
+// root's neighbours), so no frontier queue -- and no more scratch -- is
+// needed.  The host reads the level's count after each level, so the call
+// synchronises its stream once per level; a stream that is being captured
+// into a CUDA graph is refused before anything is enqueued on it.
 #include <algorithm>
 #include <mutex>
 #include "common.cuh"
@@ -132,6 +136,18 @@ extern "C" int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, i
   if (!row_ptr || !col || !pred) return B200BFS_ERR_INVALID;
   if (nrows < 1 || nrows > kMaxRows) return B200BFS_ERR_INVALID;  // beyond the fixed scratch
   if (root < 0 || root >= nrows) return B200BFS_ERR_INVALID;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  {
+    // The per-level readback and synchronisation are not allowed during
+    // stream capture: refuse before enqueuing anything, so that the caller's
+    // capture stays intact.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+      cudaGetLastError();
+      return B200BFS_ERR_INVALID;
+    }
+    if (cs != cudaStreamCaptureStatusNone) return B200BFS_ERR_INVALID;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
     cudaGetLastError();
@@ -153,7 +169,6 @@ extern "C" int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, i
     }
     scratch = g_scratch[dev].ptr;
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int64_t W = (nrows + 31) / 32;
   uint32_t* vis[2] = {scratch, scratch + kMaxWords};
   unsigned long long* found = reinterpret_cast<unsigned long long*>(scratch + 2 * kMaxWords);
@@ -163,6 +178,7 @@ extern "C" int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, i
   noalloc_init_kernel<<<grid_for(std::max(nrows, W), B, sms, 8), B, 0, s>>>(pred, nrows, vis[0],
                                                                           vis[1], W);
   noalloc_root_kernel<<<1, 1, 0, s>>>(pred, vis[0], vis[1], root);
+  if (cudaGetLastError() != cudaSuccess) return B200BFS_ERR_CUDA;
   int cur = 0;
   int64_t level = 0;
   for (;;) {
@@ -171,6 +187,9 @@ extern "C" int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, i
     if (cudaMemsetAsync(found, 0, sizeof(unsigned long long), s) != cudaSuccess) break;
     noalloc_bu_kernel<<<grid_for(W * 32, B, sms, 8), B, 0, s>>>(vis[cur], vis[cur ^ 1], W, row_ptr,
                                                                 col, pred, level, nrows, found);
+    // a launch that failed would leave the count at 0 and end the search
+    // early with a partial pred: report it instead
+    if (cudaGetLastError() != cudaSuccess) return B200BFS_ERR_CUDA;
     unsigned long long h = 0;
     if (cudaMemcpyAsync(&h, found, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess) break;
     if (cudaStreamSynchronize(s) != cudaSuccess) break;

@@ -1,7 +1,8 @@
 // Graph500 result validation on the device.
 //
-// Restates BfsValidation::validate (mpi/validate.hpp:607-976) for one GPU:
-// value ranges (:994-1016), root is its own parent, no other self-parent,
+// Restates BfsValidation::validate (mpi/validate.hpp:607-976) for one GPU,
+// stopping at the first group of checks that finds errors, as the reference
+// does: value ranges (:994-1016), root is its own parent, no other self-parent,
 // the depth map (check_bfs_depth_map_using_predecessors :1145-1254, or
 // build_bfs_depth_map :1040-1141 with CoreBFS, which leaves tree levels
 // unknown), then one pass over the input edges: endpoint depths must differ
@@ -33,14 +34,22 @@ __global__ void max_used_kernel(const uint8_t* __restrict__ has, int64_t n,
 }
 
 __global__ void range_kernel(const int64_t* __restrict__ pred, int64_t n, int64_t nglobal,
-                             int64_t root, unsigned long long* err) {
+                             unsigned long long* err) {
   unsigned long long e = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = parent_of(pred[i]);
     if (p < -1 || p >= nglobal) ++e;
-    else if (i != root && p != -1 && p == i) ++e;
   }
+  if (e) atomicAdd(err, e);
+}
+
+__global__ void self_parent_kernel(const int64_t* __restrict__ pred, int64_t n, int64_t root,
+                                   unsigned long long* err) {
+  unsigned long long e = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (i != root && parent_of(pred[i]) == i) ++e;
   if (e) atomicAdd(err, e);
 }
 
@@ -138,7 +147,8 @@ __global__ void set_root_depth_kernel(int64_t* pred, int64_t root) {
 }  // namespace
 
 void validate_device(DeviceArena& arena, cudaStream_t s, int sms, const Graph& g,
-                     const BfsState& st, int64_t root, int64_t* errors, int64_t* edge_visit_count) {
+                     const int64_t* pred, bool corebfs, int64_t root, int64_t* errors,
+                     int64_t* edge_visit_count) {
   const int B = 256;
   const int64_t n = g.pred_size;
   auto grid = [&](int64_t items) { return grid_for(items, B, sms, 16); };
@@ -157,17 +167,34 @@ void validate_device(DeviceArena& arena, cudaStream_t s, int sms, const Graph& g
   const int64_t nglobal = (int64_t)maxv + 1;
 
   int64_t* p = arena_alloc<int64_t>(arena, n, "pred copy");
-  check_cuda(cudaMemcpyAsync(p, st.pred, n * 8, cudaMemcpyDeviceToDevice, s), "copy");
-  range_kernel<<<grid(n), B, 0, s>>>(p, n, nglobal, root, cnt);
-  int64_t proot = 0;
-  check_cuda(cudaMemcpyAsync(&proot, p + root, 8, cudaMemcpyDeviceToHost, s), "copy");
-  unsigned long long herr = 0;
-  check_cuda(cudaMemcpyAsync(&herr, cnt, 8, cudaMemcpyDeviceToHost, s), "copy");
-  check_cuda(cudaStreamSynchronize(s), "validate ranges");
-  const int64_t root_parent = (int64_t)((uint64_t)proot << 16) >> 16;
-  int64_t err = (int64_t)herr + (root_parent != root ? 1 : 0);
+  check_cuda(cudaMemcpyAsync(p, pred, n * 8, cudaMemcpyDefault, s), "copy");
+  // The checks run in the reference's order and stop at the first that
+  // fails (validate.hpp:612-664): value ranges, the root's own parent,
+  // other self-parents, the depth map, then the pass over the input edges.
+  auto read_errors = [&](const char* what) {
+    unsigned long long h = 0;
+    check_cuda(cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, s), "copy");
+    check_cuda(cudaStreamSynchronize(s), what);
+    return (int64_t)h;
+  };
+  *edge_visit_count = 0;
+  range_kernel<<<grid(n), B, 0, s>>>(p, n, nglobal, cnt);
+  // a root beyond the used vertex range counts as one more range error
+  int64_t err = read_errors("validate ranges") + (root >= nglobal ? 1 : 0);
   if (err == 0) {
-    if (g.core.enabled) {
+    int64_t proot = 0;
+    check_cuda(cudaMemcpyAsync(&proot, p + root, 8, cudaMemcpyDeviceToHost, s), "copy");
+    check_cuda(cudaStreamSynchronize(s), "root entry");
+    if (((int64_t)((uint64_t)proot << 16) >> 16) != root) err = 1;
+  }
+  if (err == 0) {
+    self_parent_kernel<<<grid(n), B, 0, s>>>(p, n, root, cnt);
+    err = read_errors("validate self parents");
+  }
+  if (err == 0) {
+    if (corebfs) {
+      // build_bfs_depth_map (validate.hpp:1040-1141): tree entries take
+      // their parent's depth + 1; it reports no errors of its own
       set_root_depth_kernel<<<1, 1, 0, s>>>(p, root);
       int* changed = arena_alloc<int>(arena, 1, "flag");
       for (int pass = 0; pass < 0x10000; ++pass) {
@@ -181,7 +208,10 @@ void validate_device(DeviceArena& arena, cudaStream_t s, int sms, const Graph& g
       arena.free(changed);
     } else {
       depth_check_kernel<<<grid(n), B, 0, s>>>(p, n, root, cnt);
+      err = read_errors("validate depth map");
     }
+  }
+  if (err == 0) {
     uint8_t* valid = arena_alloc<uint8_t>(arena, n, "pred valid");
     check_cuda(cudaMemsetAsync(valid, 0, n, s), "memset");
     edge_check_kernel<<<grid(g.num_input_edges), B, 0, s>>>(g.input_edges, g.num_input_edges, n,
@@ -193,8 +223,6 @@ void validate_device(DeviceArena& arena, cudaStream_t s, int sms, const Graph& g
     arena.free(valid);
     err = (int64_t)h2[0];
     *edge_visit_count = (int64_t)h2[1];
-  } else {
-    *edge_visit_count = 0;
   }
   *errors = err;
   arena.free(p);

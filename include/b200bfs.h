@@ -320,6 +320,16 @@ int b200bfs_end(b200bfs_handle* h);
 int b200bfs_validate(b200bfs_handle* h, int64_t root, int64_t* errors,
                      int64_t* edge_visit_count);
 
+/* Replaces validate_bfs_result (validate.hpp:1269-1277, called by main.cc:647)
+ * for a pred the caller holds: the same Graph500 rules as b200bfs_validate,
+ * applied to pred[pred_size] (host or device memory, read only) from root
+ * against the graph's resident input edges.  corebfs != 0 selects the
+ * CoreBFS mode of the reference (tree entries with level 0xFFFF, depths
+ * rebuilt from parents).  Needs a built graph, not a search; *errors is 0
+ * for a valid pred. */
+int b200bfs_validate_pred(b200bfs_handle* h, int64_t root, const int64_t* pred, int corebfs,
+                          int64_t* errors, int64_t* edge_visit_count);
+
 /* ---------------------------- batched search ------------------------------ */
 
 #define B200BFS_BATCH_MAX 64
@@ -443,21 +453,29 @@ int b200bfs_server_stop(b200bfs_server* srv);
 #define B200BFS_NOALLOC_MAX_ROWS (1 << 24)
 
 /* No counterpart in the reference: an entry point for callers that may not
- * allocate device memory -- code running under CUDA graph capture, programs
- * whose memory pool owns the whole device, hosts with a fixed budget.  It
- * searches a CSR the caller already holds on the device (row_ptr[nrows + 1]
- * int64, col[row_ptr[nrows]] int32 row ids, rows sorted or not) from `root`
- * and writes pred[nrows] (device memory, same encoding as pred above with row
- * ids as vertex ids, -1 unreached); *num_levels (host, may be NULL) receives
- * the last level, as AUTO_LEVEL.  stream is a cudaStream_t (NULL = legacy
- * default stream); the call returns once the search is complete.
+ * allocate device memory -- applications whose caching allocator owns the
+ * device memory (a framework's pool that must not be bypassed) and hosts that
+ * give the library a fixed memory budget at start-up.  It searches a CSR the
+ * caller already holds on the device (row_ptr[nrows + 1] int64,
+ * col[row_ptr[nrows]] int32 row ids, rows sorted or not) from `root` and
+ * writes pred[nrows] (device memory, same encoding as pred above with row ids
+ * as vertex ids, -1 unreached); *num_levels (host, may be NULL) receives the
+ * last level, as AUTO_LEVEL.  The CSR must be symmetric (every edge stored
+ * in both directions, as the engine's own CSR is): the search is bottom-up
+ * only and takes any neighbour visited before a level as the parent, which
+ * gives BFS levels only on an undirected graph.  Column ids outside
+ * [0, nrows) are ignored.  stream is a cudaStream_t (NULL = legacy default
+ * stream); the host reads a counter after every level, so the call
+ * synchronises the stream once per level and returns once the search is
+ * complete; a stream that is being captured is refused with
+ * B200BFS_ERR_INVALID before anything is enqueued.
  * It allocates nothing: its scratch (two visited bitmaps and a counter) lives
  * in one fixed device array of B200BFS_NOALLOC_MAX_ROWS / 4 bytes that every
  * GPU loading the library keeps until exit.  Graphs with more rows are
  * rejected with B200BFS_ERR_INVALID.  The first call on a device looks up
- * that array's device address, so make it before capturing a stream into a
- * graph.  All calls share the array: calls that overlap on the GPU (other
- * threads or streams) race and must be serialised by the caller. */
+ * that array's device address.  All calls share the array: calls that overlap
+ * on the GPU (other threads or streams) race and must be serialised by the
+ * caller. */
 int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, int64_t nrows,
                         int64_t root, int64_t* pred, void* stream, int32_t* num_levels);
 

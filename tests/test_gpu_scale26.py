@@ -2,12 +2,15 @@
 switch points, and -A -C (CoreBFS) with group reordering -- plus a 64-root
 batch on the same graph.
 
-At this size the CPU oracle is too slow to run here, so parity rests on
-size-independent properties: per-vertex levels depend only on the graph and
-the root, so all four ways must give identical levels; every parent array
-must pass the Graph500 rules on the device; and the traversed-edge count of
-every root in the giant component equals the reference's known answer
-pf_nedge[26] (mpi/utils.hpp:3687-3733).
+Anchors: the CPU oracle generates the SCALE 26 graph itself on the host
+(about 50 GB of host memory, a minute or two on the box's cores), builds its
+own CSR and searches it; the engine's CSR sizes, root sample, per-vertex
+levels and auto_tuning_data slots (plain α/β) must equal the oracle's for
+the first roots, and the device validator's traversed-edge count must equal
+the oracle validator's.  Levels depend only on the graph and the root, so the
+-A, -A -C (group reordering) and batched searches must give the same levels
+again; every parent array passes the Graph500 rules on the device with the
+reference's known answer pf_nedge[26] (mpi/utils.hpp:3687-3733).
 """
 import numpy as np
 import pytest
@@ -18,6 +21,7 @@ pytestmark = pytest.mark.gpu
 
 SCALE = 26
 NROOTS = 8
+NORACLE = 4  # roots also searched by the CPU oracle
 
 
 @pytest.fixture(scope="module")
@@ -52,6 +56,38 @@ def plain_levels(built):
         assert err == 0 and cnt == O.PF_NEDGE[SCALE]
     e.close()
     return roots, levels
+
+
+@pytest.fixture(scope="module")
+def oracle26(plain_levels):
+    """The oracle's own graph, generated and built on the host."""
+    edges = O.generate_edges(SCALE)
+    g = O.Graph(edges)
+    yield edges, g
+    del g, edges
+
+
+def test_scale26_matches_oracle_graph(plain_levels, oracle26):
+    import b200bfs
+
+    roots, levels = plain_levels
+    edges, g = oracle26
+    e = b200bfs.Engine(0)
+    e.generate_graph(SCALE, 16)
+    gi = e.info()
+    assert gi.num_global_edges == g.num_edges and gi.num_global_verts == g.num_verts
+    e.prepare(16)
+    assert np.array_equal(e.find_roots(NROOTS), O.find_roots(g.has_edge(), 1 << SCALE, NROOTS))
+    n = 1 << SCALE
+    for r in roots[:NORACLE]:
+        at = e.run(r, 16)
+        pred, ref_at, _ = g.bfs(r)
+        assert np.array_equal(at, ref_at), (r, at, ref_at)
+        assert np.array_equal(levels[r][:n], O.pred_levels(pred)), r
+        err, cnt = O.validate(edges, n, e.get_pred()[:n], r)
+        assert err == 0 and cnt == O.PF_NEDGE[SCALE], r
+        assert e.validate(r) == (0, cnt)
+    e.close()
 
 
 def test_scale26_plain_tuned_and_batch(plain_levels):

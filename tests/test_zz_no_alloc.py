@@ -1,9 +1,11 @@
 """b200bfs_bfs_noalloc: the search entry point for callers that may not
-allocate device memory (code under CUDA graph capture, programs whose memory
-pool owns the device, fixed-budget hosts).  Its scratch lives in a fixed
-device array inside the library, so the test hands it only device inputs and
-outputs and checks its results against the engine's own b200bfs_run on the
-same graph, on two calls in a row.  This file sorts last so that a run
+allocate device memory (programs whose caching allocator owns the device,
+hosts with a fixed memory budget).  Its scratch lives in a fixed device array
+inside the library, so the test hands it only device inputs and outputs and
+checks its results against the engine's own b200bfs_run on the same graph,
+on two calls in a row.  It synchronises its stream once per level, so a
+stream being captured into a CUDA graph is refused before anything is
+enqueued, and the capture stays usable.  This file sorts last so that a run
 stopping at the first failure has already run every other test."""
 import numpy as np
 import pytest
@@ -61,3 +63,31 @@ def test_noalloc_rejects_too_large(built):
         b200bfs.bfs_noalloc(dummy.data_ptr(), dummy.data_ptr(), b200bfs.NOALLOC_MAX_ROWS + 1, 0,
                             dummy.data_ptr())
     assert ei.value.code == 1
+
+
+def test_noalloc_refuses_capturing_stream(built):
+    import torch
+    import b200bfs
+
+    row_ptr = torch.tensor([0, 1, 2], dtype=torch.int64, device="cuda")
+    col = torch.tensor([1, 0], dtype=torch.int32, device="cuda")
+    pred = torch.empty(2, dtype=torch.int64, device="cuda")
+    x = torch.zeros(4, device="cuda")
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    codes = []
+    with torch.cuda.graph(g, stream=s):
+        x.add_(1)
+        try:
+            b200bfs.bfs_noalloc(row_ptr.data_ptr(), col.data_ptr(), 2, 0, pred.data_ptr(),
+                                stream=s.cuda_stream)
+        except b200bfs.B200BfsError as e:
+            codes.append(e.code)
+        x.add_(1)
+    assert codes == [1]  # B200BFS_ERR_INVALID, nothing enqueued
+    g.replay()
+    torch.cuda.synchronize()
+    assert x.tolist() == [2.0] * 4  # the capture was not broken
+    # outside a capture the same call searches
+    assert b200bfs.bfs_noalloc(row_ptr.data_ptr(), col.data_ptr(), 2, 0, pred.data_ptr()) == 2
+    assert pred.cpu().tolist() == [0, (1 << 48) | 0]
