@@ -74,6 +74,10 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--cpu-sample-sec", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-scale", type=int, default=22,
+                   help="SCALE of the reference arm (--impl reference): the reference's own "
+                        "CPU program cannot build the SCALE 28 graph on this host")
+    p.add_argument("--ref-timeout", type=float, default=1800.0)
     return p.parse_args()
 
 
@@ -445,48 +449,110 @@ def workload_config(args):
             "parallelism": "replicas"}
 
 
+def host_facts():
+    """Cores, CPU model and memory of this host (the CPU reference's machine)."""
+    model, mem_gb = None, None
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemTotal"):
+                mem_gb = int(ln.split()[1]) / 1e6
+                break
+    except OSError:
+        pass
+    return {"cores": os.cpu_count(), "cpu": model, "mem_gb": mem_gb}
+
+
 def run_reference(args, rank, world, dist):
-    """The reference arm: the reference algorithm (CPU restatement in oracle/)
-    on the host cores, same graph, metric and unit."""
+    """The reference arm: the reference's own CPU BFS, i.e. mpi/main.cc with
+    its stock BfsBase compiled unchanged against the single-rank MPI runtime
+    (oracle/_ref/ref_runnable[_group], built by oracle/ref/Makefile), run as
+    `mpiexec -n 1 runnable SCALE [-A] [-C] -n K -v 1` on all host cores.  No
+    library of this repository is loaded in the process that runs it.
+
+    SCALE is --ref-scale (default 22), not the GPU arm's 28: the reference
+    keeps the edge lists and a 64-bit edge array in host memory (about
+    225 GB at SCALE 28, more than this host's 196 GB), and its single-process
+    CoreBFS construction takes 213 s at SCALE 22 and 861 s at SCALE 24 on the
+    16 host cores, about an hour at SCALE 26.  The options are the GPU arm's
+    (-A tuner, -C CoreBFS, group reordering).  Warm-up: W extra roots whose
+    searches are dropped; value = harmonic-mean TEPS of the next K roots from
+    the reference's own per-root "Time for BFS" and traversed-edge lines."""
     if rank != 0:
         return
-    import b200bfs
+    import re
 
+    scale = args.ref_scale
+    exe = os.path.join(ROOT, "oracle", "_ref",
+                       "ref_runnable_group" if args.group_reorder else "ref_runnable")
+    if not os.access(exe, os.X_OK):
+        raise SystemExit(f"{exe} missing: build it with `make -C oracle/ref` where the "
+                         "reference tree is")
+    nroots = min(64, args.warmup + args.steps)
+    cmd = [exe, str(scale), "-e", str(args.edgefactor), "-n", str(nroots), "-v", "1",
+           "-r", str(args.root_seed)]
+    cmd += (["-A"] if args.auto_tune else []) + (["-C"] if args.corebfs else [])
+    if not args.auto_tune:
+        cmd += ["-a", str(args.alpha), "-b", str(args.beta)]
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
     t0 = time.time()
-    eng = b200bfs.Engine(0)
-    # the reference's plain CPU run (no -A, no -C) on the same generated graph
-    args.alpha, args.beta = 10.0, 14.0
-    eng.generate_graph(args.scale, args.edgefactor)
-    eng.prepare(args.edgefactor, args.alpha, args.beta)
-    roots, nedge = pick_roots(eng, args)
-    info = eng.info()
-    row_ptr, col, inv, mdeg = host_csr(eng)
-    eng.close()
-    log(f"graph ready for the CPU search in {time.time() - t0:.1f}s")
-    rows = rows_of(inv, roots, 1 << info.scale)
-    order = [i % len(rows) for i in range(args.warmup + args.steps)]
-    import ctypes
+    log("reference: " + " ".join(os.path.relpath(c, ROOT) if c == exe else c for c in cmd))
+    p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=args.ref_timeout)
+    out = p.stdout + "\n" + p.stderr
+    if p.returncode != 0 or "No results printed for invalid run" in out:
+        raise SystemExit(f"reference run failed (rc {p.returncode}):\n{out[-3000:]}")
+    times = {int(m.group(1)): float(m.group(2))
+             for m in re.finditer(r"Time for BFS (\d+) is ([0-9.eE+-]+)", out)}
+    # traversed-edge lines carry no index; they follow the roots in order
+    counts = [int(m.group(1)) for m in re.finditer(r"Number of traversed edges is (\d+)", out)]
+    idx = sorted(times)
+    if len(idx) != nroots or len(counts) != nroots:
+        raise SystemExit(f"reference output has {len(idx)} timed searches, {len(counts)} edge "
+                         f"counts, expected {nroots}")
+    keep = idx[args.warmup:] if nroots > args.warmup else idx
+    t = [times[i] for i in keep]
+    used = [counts[idx.index(i)] for i in keep]
+    value = harmonic_teps(used, t) / 1e9
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    times_w, _, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size,
-                                          rows[order[: args.warmup]], nedge[order[: args.warmup]],
-                                          args, 1e9)
-    steps = order[args.warmup:]
-    times, used, cores = cpu_search_sample(row_ptr, col, mdeg, inv, info.pred_size, rows[steps],
-                                           nedge[steps], args, 1e9)
-    value = harmonic_teps(used, times) / 1e9
+    def field(name):
+        m = re.search(r"^%s:\s+(\S+)" % name, out, re.M)
+        return float(m.group(1)) if m else None
+
+    cfg = {
+        "workload": f"Graph500 Kronecker SCALE {scale} edgefactor {args.edgefactor} "
+                    f"(A,B,C=.57,.19,.19, seeds 2/3), {len(keep)} roots, the reference's own "
+                    "single-source direction-optimizing BFS on the host CPU, "
+                    + " ".join(x for x, on in (("-A", args.auto_tune), ("-C", args.corebfs),
+                                               ("group reordering", args.group_reorder)) if on),
+        "auto_tune": bool(args.auto_tune), "scale": scale, "edgefactor": args.edgefactor,
+        "roots": len(keep), "corebfs": bool(args.corebfs),
+        "group_reorder": bool(args.group_reorder),
+        "alpha": field("alpha"), "beta": field("beta"),
+        "gpu_arm_scale": args.scale,
+        "why_not_gpu_arm_scale": "the reference needs about 225 GB of host memory at SCALE 28 "
+                                 "(this host has %.0f GB) and about an hour of single-process "
+                                 "CoreBFS construction at SCALE 26" % (host_facts()["mem_gb"] or 0),
+        "construction_s": field("construction_time"),
+        "host": host_facts(),
+        "parallelism": "one process, OpenMP on all host cores (mpiexec -n 1)",
+    }
+    sample = (f"{len(keep)} searches at SCALE {scale} (after {nroots - len(keep)} warm-up "
+              f"searches) by the reference's mpi/main.cc + BfsBase, compiled unchanged "
+              f"(GNU3 flags, single-rank MPI runtime), {time.time() - t0:.0f} s in all")
     line = {
         "impl": "reference",
         "metric": f"harmonic-mean GTEPS, SCALE {args.scale}; 64-root batched BFS/s + p99 vs 1-root",
-        "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "value": value, "unit": "GTEPS", "n_gpus": world, "steps": len(keep),
+        "warmup": nroots - len(keep), "ms_per_step": 1e3 * float(np.mean(t)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (Graph500 Kronecker generator, seeds 2/3)",
-        "config": workload_config(args),
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
-                         "sample": f"{len(times)} searches at SCALE {args.scale} with the "
-                                   "oracle's OpenMP restatement of BfsBase::run_bfs_core "
-                                   "(graph built on the GPU and copied to host memory)"},
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

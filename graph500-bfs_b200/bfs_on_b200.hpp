@@ -190,6 +190,13 @@ class BfsOnB200 {
 #endif
     for (int64_t v = 0; v < n; ++v)
       if (has_edge_[(size_t)v]) g.has_edge_bitmap_[v >> 6] |= BitmapType(1) << (v & 63);
+#ifdef BFS_HPP_
+    // main.cc:519-533 reports the all-to-all buffer sizes in units of the
+    // global a2a_buf_unit (it divides by it), which BfsBase sets when it
+    // allocates (bfs.hpp:218).  The engine uses no such buffers, so
+    // max_num_buffers stays 0 and the proposed size printed is 0.
+    a2a_buf_unit = g.num_local_verts_ * (int64_t)sizeof(int32_t);
+#endif
   }
 #else
   void fill_graph(const b200bfs_graph_info& gi) {

@@ -39,7 +39,10 @@ def test_device_validator_matches_oracle(built, scale, corebfs, group):
     pred = e.get_pred()
     cases = [("valid", pred)] + list(corruptions(pred, root, g.row_ptr, g.col, nglobal,
                                                  corebfs=corebfs))
-    assert len(cases) >= (9 if corebfs else 8), [c[0] for c in cases]
+    # one case per rule; a vertex with edges that the search does not reach
+    # (needed for "unreachable_marked_reached") exists only on some graphs
+    unreached = ((pred[:nglobal] == -1) & (np.diff(g.row_ptr)[:nglobal] > 0)).any()
+    assert len(cases) == 7 + int(bool(unreached)) + (2 if corebfs else 0), [c[0] for c in cases]
     for name, p in cases:
         derr, dcnt = e.validate_pred(root, p, corebfs=corebfs)
         oerr, ocnt = O.validate(edges, nglobal, p, root, corebfs=corebfs, nlocalverts=pred_size)
