@@ -455,3 +455,16 @@ def test_pred_exact_across_searches(engine, oracle_graphs, single_graph, assembl
         engine.set_option("single_graph", 0)
         engine.set_option("pred_assemble", 1)
         engine.end()
+
+
+@pytest.mark.parametrize("scale,flags", [(16, 0), (20, 2)])
+def test_find_roots_matches_oracle(engine, oracle_graphs, scale, flags):
+    """b200bfs_find_roots against the oracle's find_roots
+    (benchmark_helper.hpp:527-562) for several seeds, plain and with group
+    reordering (has_edge is by original id either way)."""
+    edges, g = oracle_graphs(scale)
+    engine.generate_graph(scale, 16, flags=flags)
+    for r1, r2 in ((0, 0), (1, 0), (2, 0), (5, 3), (17, 0)):
+        dev = engine.find_roots(16, r1, r2)
+        ref = O.find_roots(g.has_edge(), 1 << scale, 16, r1, r2)
+        assert np.array_equal(dev, ref), (r1, r2)

@@ -91,3 +91,26 @@ def test_noalloc_refuses_capturing_stream(built):
     # outside a capture the same call searches
     assert b200bfs.bfs_noalloc(row_ptr.data_ptr(), col.data_ptr(), 2, 0, pred.data_ptr()) == 2
     assert pred.cpu().tolist() == [0, (1 << 48) | 0]
+
+
+def test_noalloc_level_overflow_is_an_error(built):
+    import torch
+    import b200bfs
+
+    n = 70000  # a path searched from one end: 69,999 levels > 0xFFFE
+    v = np.arange(n, dtype=np.int64)
+    row_ptr = np.concatenate([[0], np.cumsum(np.where((v == 0) | (v == n - 1), 1, 2))])
+    col = np.empty(row_ptr[-1], np.int32)
+    for_left = v[1:]
+    col[row_ptr[for_left]] = (for_left - 1).astype(np.int32)  # first neighbour: v - 1
+    right = v[:-1]
+    col[row_ptr[right + 1] - 1] = (right + 1).astype(np.int32)  # last neighbour: v + 1
+    d_row = torch.from_numpy(row_ptr).cuda()
+    d_col = torch.from_numpy(col).cuda()
+    d_pred = torch.empty(n, dtype=torch.int64, device="cuda")
+    with pytest.raises(b200bfs.B200BfsError) as ei:
+        b200bfs.bfs_noalloc(d_row.data_ptr(), d_col.data_ptr(), n, 0, d_pred.data_ptr())
+    assert ei.value.code == 6  # B200BFS_ERR_OVERFLOW
+    # from the middle the same call searches the whole path
+    assert b200bfs.bfs_noalloc(d_row.data_ptr(), d_col.data_ptr(), n, n // 2,
+                               d_pred.data_ptr()) == n // 2 + 1
