@@ -739,6 +739,121 @@ __device__ __forceinline__ void td_chunk_body(
   }
 }
 
+// Top-down expansion, vector form.  Edge-balanced over the concatenated
+// frontier rows like td_expand_body, in tiles of kVecTile entries strided
+// over the warps, but a warp advances 128 entries per step: when the whole
+// step lies inside one row (the hub rows that carry almost all entries of a
+// heavy top-down level), each lane takes four consecutive neighbours with one
+// 16-byte load (four 4-byte loads when the address is not 16-byte aligned),
+// issues their four visited probes together and claims the unvisited ones;
+// the row, its column offset and the parent's pred entry are warp-uniform,
+// so the step costs no per-entry row lookup.  A step that crosses a row
+// boundary runs as four 32-entry sub-steps with the per-lane row walk of
+// td_expand_body; its last row, taken from lane 31, becomes the warp's row
+// for the next step.
+constexpr int kVecTile = 1024;  // entries per warp tile: 8 steps of 128
+
+__device__ __forceinline__ void td_claim(int32_t u, uint32_t word, int64_t entry,
+                                         const int32_t* __restrict__ pidx, uint32_t* vis,
+                                         int64_t* __restrict__ pred) {
+  const uint32_t bit = 1u << (u & 31);
+  if ((word & bit) == 0) {
+    pred[pred_slot(pidx, u)] = entry;
+    red_or(vis + (u >> 5), bit);
+  }
+}
+
+__device__ __forceinline__ void td_vec_body(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  const int64_t qsize = (int64_t)ctr->qsize;
+  if (qsize == 0) return;
+  const int64_t total = qdeg[qsize];
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (total + kVecTile - 1) / kVecTile;
+  for (int64_t tile = gw; tile < ntiles; tile += nwarps) {
+    const int64_t t0 = tile * kVecTile;
+    const int64_t t_end = min(total, t0 + kVecTile);
+    // warp-uniform row state: row i of the queue holds entries [seg_lo, seg_hi)
+    int64_t i = warp_segment_search(qdeg, 0, qsize - 1, t0);
+    int64_t seg_lo = qdeg[i], seg_hi = qdeg[i + 1];
+    int32_t src = queue[i];
+    int64_t rbeg = row_ptr[src];
+    int64_t entry = pred_entry(__ldg(inv + src), level);
+    for (int64_t e0 = t0; e0 < t_end; e0 += 128) {
+      while (e0 >= seg_hi && i + 1 < qsize) {  // rows ending before the step
+        ++i;
+        seg_lo = seg_hi;
+        seg_hi = qdeg[i + 1];
+        src = queue[i];
+        rbeg = row_ptr[src];
+        entry = pred_entry(__ldg(inv + src), level);
+      }
+      if (e0 + 128 <= seg_hi && e0 + 128 <= t_end) {
+        // the whole step is in row i: col[base .. base + 3] for this lane
+        const int32_t* p = col + rbeg + (e0 - seg_lo) + 4 * lane;
+        int32_t u0, u1, u2, u3;
+        if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+          const int4 v = __ldg(reinterpret_cast<const int4*>(p));
+          u0 = v.x;
+          u1 = v.y;
+          u2 = v.z;
+          u3 = v.w;
+        } else {
+          u0 = __ldg(p);
+          u1 = __ldg(p + 1);
+          u2 = __ldg(p + 2);
+          u3 = __ldg(p + 3);
+        }
+        // plain loads: vis is being updated by this kernel; a stale word
+        // only causes a redundant (still valid) claim
+        const uint32_t w0 = vis[u0 >> 5], w1 = vis[u1 >> 5], w2 = vis[u2 >> 5],
+                       w3 = vis[u3 >> 5];
+        td_claim(u0, w0, entry, pidx, vis, pred);
+        td_claim(u1, w1, entry, pidx, vis, pred);
+        td_claim(u2, w2, entry, pidx, vis, pred);
+        td_claim(u3, w3, entry, pidx, vis, pred);
+        continue;
+      }
+      // the step crosses a row boundary: per-lane walk over 32-entry sub-steps
+      int64_t li = i, l_lo = seg_lo, l_hi = seg_hi, l_rb = rbeg;
+      int32_t l_src = src;
+      const int64_t step_end = min(e0 + 128, t_end);
+#pragma unroll 1
+      for (int k = 0; k < 4; ++k) {
+        const int64_t e = e0 + k * 32 + lane;
+        if (e < step_end) {
+          while (e >= l_hi && li + 1 < qsize) {
+            ++li;
+            l_lo = l_hi;
+            l_hi = qdeg[li + 1];
+            l_src = queue[li];
+            l_rb = row_ptr[l_src];
+          }
+          const int32_t u = __ldg(col + l_rb + (e - l_lo));
+          td_claim(u, vis[u >> 5], pred_entry(__ldg(inv + l_src), level), pidx, vis, pred);
+        }
+      }
+      // lane 31 walked furthest (to the row of entry e0 + 127, when the tile
+      // reaches it); the next step starts from there
+      const int64_t ni = __shfl_sync(kFull, li, 31);
+      if (ni != i) {
+        i = ni;
+        seg_lo = qdeg[i];
+        seg_hi = qdeg[i + 1];
+        src = queue[i];
+        rbeg = row_ptr[src];
+        entry = pred_entry(__ldg(inv + src), level);
+      }
+    }
+  }
+}
+
 // Frontier pass 1: fr = nw & ~old, old = nw; per-block counts of frontier
 // vertices, their CSR degrees and their pre-dedup degrees.
 // kDeg: also the per-block CSR degree sums of the frontier, which only a
@@ -975,6 +1090,15 @@ __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
   bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred, level,
                                ctr);
   publish_if_last(ctr, pub, seq);
+}
+
+__global__ void __launch_bounds__(256) td_vec_kernel(
+    const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
+    const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, uint32_t* vis,
+    int64_t* __restrict__ pred, int64_t level) {
+  td_vec_body(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
@@ -1596,7 +1720,8 @@ static Counters wait_level(BfsState& st, cudaStream_t s) {
 void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                   int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
                   const RunOptions& opt, b200bfs_run_stats* stats) {
-  if (opt.single_graph && opt.bu_kernel == 4 && opt.td_kernel != 2) {
+  // the device-driven loop has top-down forms 1, 3, 4 and 5
+  if (opt.single_graph && opt.bu_kernel == 4 && opt.td_kernel != 2 && opt.td_kernel <= 5) {
     run_bfs_core_graph(g, st, s, sms, root, root_level, edgefactor, alpha, beta, at, opt, stats);
     return;
   }
@@ -1654,7 +1779,9 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // form 4: the strided form while the frontier grows (hub rows), the
       // chunked form once the search has come back from bottom-up (short
       // rows of the tail levels)
-      const int td_form = opt.td_kernel == 4 ? (growing ? 5 : 3) : opt.td_kernel;
+      const int td_form = opt.td_kernel == 4   ? (growing ? 5 : 3)
+                          : opt.td_kernel == 7 ? (growing ? 6 : 3)
+                                               : opt.td_kernel;
       // every top-down form has the same parameters
       // one resident wave of each form (their register counts differ)
       auto launch_td = [&](auto kernel, int grid) {
@@ -1662,7 +1789,9 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
         kernel<<<grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                   st.vis[cur], out, level);
       };
-      if (td_form == 5 && opt.td_unroll == 4)
+      if (td_form == 6)
+        launch_td(td_vec_kernel, 0);
+      else if (td_form == 5 && opt.td_unroll == 4)
         launch_td(td_expand_kernel<true, 4>, 0);
       else if (td_form == 5 && opt.td_unroll == 2)
         launch_td(td_expand_kernel<true, 2>, 0);

@@ -111,7 +111,9 @@ struct RunOptions {
   // Top-down form.  1: td_expand_kernel, 2: td_wide_kernel, 3: td_chunk_kernel,
   // 4: form 5 while the frontier grows, form 3 after the switch back from
   // bottom-up (measured best at SCALE 24 and 28), 5: td_expand_kernel with a
-  // warp-wide search for each tile's first row.
+  // warp-wide search for each tile's first row, 6: td_vec_kernel (128-entry
+  // warp steps, four neighbours per lane inside a row), 7: form 6 while the
+  // frontier grows, form 3 after the switch back.
   int td_kernel = 4;
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int bu_first = 1;         // bottom-up form 4: probe the dense first-neighbour array first

@@ -530,7 +530,7 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
       require(value >= 1 && value <= 4, B200BFS_ERR_INVALID, "bu_kernel must be 1..4");
       e.opt.bu_kernel = (int)value;
     } else if (n == "td_kernel") {
-      require(value >= 1 && value <= 5, B200BFS_ERR_INVALID, "td_kernel must be 1..5");
+      require(value >= 1 && value <= 7, B200BFS_ERR_INVALID, "td_kernel must be 1..7");
       e.opt.td_kernel = (int)value;
     } else if (n == "bu_first") {
       require(value == 0 || value == 1, B200BFS_ERR_INVALID, "bu_first must be 0 or 1");

@@ -85,7 +85,7 @@ extern "C" int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int 
       e.opt.bu_kernel = best_bu;
       best = 1e30;
       int best_td = e.opt.td_kernel;
-      for (int td : {1, 3, 4, 5}) {
+      for (int td : {1, 3, 4, 5, 6, 7}) {
         e.opt.td_kernel = td;
         const double t = b200bfs::time_searches(e, rs, edgefactor, alpha, beta, ev);
         rep.searches += (int)rs.size() + 1;

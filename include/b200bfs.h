@@ -280,7 +280,7 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
 
 /* Engine tuning knobs (no counterpart in the reference, whose equivalents
  * are compile-time constants of parameters.h): "bu_kernel" (1..4, bottom-up
- * kernel form), "td_kernel" (1..5, top-down kernel form; 4 picks per
+ * kernel form), "td_kernel" (1..7, top-down kernel form; 4 and 7 pick per
  * level), "bu_probe" (1..64, neighbours probed per lane by bottom-up form
  * 1), "bu_first" (1: bottom-up forms 2-4 probe the first neighbour from a
  * dense per-row array first, the default), "td_unroll" (1, 2 or 4: 32-entry

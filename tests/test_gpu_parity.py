@@ -308,7 +308,7 @@ def test_hbm_budget_admission(built):
 
 
 @pytest.mark.parametrize("bu,td,first", [(1, 1, 1), (2, 2, 1), (3, 1, 1), (4, 2, 0), (4, 3, 1),
-                                         (4, 4, 1), (4, 5, 0)])
+                                         (4, 4, 1), (4, 5, 0), (4, 6, 1), (2, 7, 1)])
 def test_kernel_forms_agree(engine, oracle_graphs, bu, td, first):
     """Every bottom-up / top-down kernel form gives the reference levels."""
     edges, g = oracle_graphs(18)
@@ -338,7 +338,7 @@ def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
     roots = O.find_roots(g.has_edge(), 1 << 18, 8)
     try:
         rep = engine.tune_engine(roots)
-        assert 1 <= rep.bu_kernel <= 4 and rep.td_kernel in (1, 3, 4, 5)
+        assert 1 <= rep.bu_kernel <= 4 and rep.td_kernel in (1, 3, 4, 5, 6, 7)
         assert rep.batch_alpha in (10.0, 20.0, 30.0, 50.0, 100.0, 200.0, 400.0)
         assert rep.searches > 0 and rep.batches == 14 and rep.single_ms > 0 and rep.batch_ms > 0
         assert (rep.alpha, rep.beta) == (10.0, 14.0)  # not refined without TUNE_SWITCH
