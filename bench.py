@@ -101,7 +101,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -213,25 +213,38 @@ def build_flags(args):
 def pick_roots(eng, args):
     """find_roots + the re-pick rule of find_roots_in_large_graph
     (main.cc:334-359): roots are drawn again with the next seed while any of
-    them reaches no more than 3 levels.  Each root's result is validated on
-    the device (validation level 2) and its traversed-edge count kept."""
+    them reaches no more than 3 levels.  The depths (AUTO_LEVEL) come from
+    one batched search per 64 roots (b200bfs_batch_root_levels, the value
+    b200bfs_run reports for each root alone).  Each root's result is then
+    validated on the device (validation level 2) and its traversed-edge count
+    kept.  Returns the roots, their counts and the time of the first
+    single-root search after prepare (pred and bitmaps cold)."""
+    import torch
+
     r = args.root_seed
     while True:
         roots = eng.find_roots(args.roots, r, 0)
-        nedge, ok = [], True
-        for root in roots:
-            at = eng.run(int(root), args.edgefactor, args.alpha, args.beta)
-            if args.scale > 6 and at[8] <= 3:
-                ok = False
-                break
-            err, cnt = eng.validate(int(root))
-            if err != 0:
-                raise RuntimeError(f"validation failed for root {root}: {err} errors")
-            nedge.append(cnt)
-        if ok:
-            return roots, np.array(nedge, dtype=np.float64)
+        depth = np.concatenate([(eng.run_batch(roots[i:i + 64], args.edgefactor, 0.0, args.beta),
+                                 eng.batch_root_levels())[1] for i in range(0, len(roots), 64)])
+        if args.scale <= 6 or (depth > 3).all():
+            break
         log(f"root seed {r}: a root reaches <= 3 levels, picking roots again")
         r += 1
+    stream = torch.cuda.ExternalStream(eng.stream())
+    nedge, cold_ms = [], None
+    for root in roots:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.run(int(root), args.edgefactor, args.alpha, args.beta)
+        b.record(stream)
+        b.synchronize()
+        if cold_ms is None:
+            cold_ms = a.elapsed_time(b)
+        err, cnt = eng.validate(int(root))
+        if err != 0:
+            raise RuntimeError(f"validation failed for root {root}: {err} errors")
+        nedge.append(cnt)
+    return roots, np.array(nedge, dtype=np.float64), cold_ms
 
 
 def harmonic_teps(nedge, times):
@@ -307,11 +320,16 @@ def percentile(x, q):
     return float(np.percentile(np.asarray(x, dtype=np.float64), q)) if len(x) else None
 
 
-def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
+def batched_leg(eng, roots, nedge, args, stream, dist, single_times, single_pred_ms):
     """64-root batched search (b200bfs_run_batch) on the same graph: BFS/s of
-    whole batches against the BFS/s of the single-source searches timed
-    above (64 sequential single-root runs), with batch latency percentiles.
-    One root of the last batch is validated on the device."""
+    whole batches against the BFS/s of 64 sequential single-root runs, with
+    batch latency percentiles.  Two baselines from the single-source searches
+    timed above: as run (b200bfs_run writes each root's complete pred, the
+    reference's output), and like for like with the batch, whose output is
+    each root's levels: the same searches without their pred assembly pass
+    (its CUDA-event time subtracted; the level kernels' row-order entries
+    then hold each row's level and parent).  One root of the last batch is
+    validated on the device."""
     import torch
 
     k = min(args.batch_roots, len(roots), 64)
@@ -355,14 +373,24 @@ def batched_leg(eng, roots, nedge, args, stream, dist, single_times):
                           "bfs_per_s": (dist.get_world_size() if dist else 1) * kk / tk})
     t_batch = barrier_max(dist, float(np.median(times)))
     t_single = barrier_max(dist, float(np.mean(single_times)))
+    t_single_lo = barrier_max(dist, float(np.mean(np.asarray(single_times)
+                                                  - np.asarray(single_pred_ms) / 1e3)))
     world = dist.get_world_size() if dist is not None else 1
     bfs_s = world * k / t_batch
     seq_bfs_s = world / t_single
+    seq_lo_bfs_s = world / t_single_lo
     sub_nedge = [nedge[idx[int(r)]] for r in np.roll(roots, 0)[:k]]
     return {
         "roots_per_batch": k, "batches": args.batch_steps,
         "bfs_per_s": bfs_s, "sequential_single_root_bfs_per_s": seq_bfs_s,
         "speedup_vs_sequential": bfs_s / seq_bfs_s,
+        "sequential_levels_only_bfs_per_s": seq_lo_bfs_s,
+        "speedup_vs_sequential_levels_only": bfs_s / seq_lo_bfs_s,
+        "baseline_definition": (
+            "speedup_vs_sequential: against 64 sequential b200bfs_run searches, each writing its "
+            "root's complete pred (2^SCALE int64 entries), as BfsBase::run_bfs does; "
+            "speedup_vs_sequential_levels_only: against the same searches without the pred "
+            "assembly pass, producing each root's levels like the batch"),
         "aggregate_gteps": world * float(np.sum(sub_nedge)) / t_batch / 1e9,
         "batch_ms_p50": 1e3 * percentile(times, 50), "batch_ms_p99": 1e3 * percentile(times, 99),
         "single_root_ms_p50": 1e3 * percentile(single_times, 50),
@@ -580,8 +608,9 @@ def main():
     log(f"[rank {rank}] graph: SCALE {info.scale}, {info.num_global_verts} vertices, "
         f"{info.num_global_edges} directed edges, built in {t_build:.1f}s, "
         f"{info.device_bytes / 1e9:.1f} GB on device")
-    roots, nedge = pick_roots(eng, args)
-    log(f"[rank {rank}] roots validated; nedge {int(nedge.min())}..{int(nedge.max())}")
+    roots, nedge, cold_ms = pick_roots(eng, args)
+    log(f"[rank {rank}] roots validated; nedge {int(nedge.min())}..{int(nedge.max())}; "
+        f"first search after prepare {cold_ms:.3f} ms")
     if args.auto_tune:
         t0 = time.time()
         args.alpha, args.beta, _ = eng.auto_tune(roots, nedge, args.edgefactor, args.alpha,
@@ -629,7 +658,6 @@ def main():
     used = [nedge[i] for i in order[args.warmup:]]
     if dist is not None:
         dist.barrier()
-    clk = clocks.stop()
     total = barrier_max(dist, sum(times))
     local_teps = harmonic_teps(used, times)
     # all replicas process the same roots: whole-job rate = sum over ranks at
@@ -649,11 +677,16 @@ def main():
         ev2[k][1].record(stream)
     torch.cuda.synchronize()
     times2 = [a.elapsed_time(b) / 1e3 for a, b in ev2]
+    # clocks sampled from the start of the device-timed searches to the end
+    # of the end-to-end ones (the device-timed region alone is shorter than
+    # the sampling interval)
+    clk = clocks.stop()
     total2 = barrier_max(dist, sum(times2))
     e2e = barrier_sum(dist, harmonic_teps(used, times2) * sum(times2)) / total2 / 1e9
 
     # ---- batched multi-source search on the same graph ----
-    batched = batched_leg(eng, roots, nedge, args, stream, dist, times)
+    batched = batched_leg(eng, roots, nedge, args, stream, dist, times,
+                          [st.pred_ms for st in stats])
 
     # ---- roofline of the dominant kernel ----
     td_ms = sum(s.td_ms for s in stats)
@@ -710,6 +743,7 @@ def main():
                    "levels": int(np.median([s.levels for s in stats])),
                    "td_ms": td_ms / args.steps, "bu_ms": bu_ms / args.steps,
                    "pred_ms": pred_ms / args.steps,
+                   "first_search_after_prepare_ms": cold_ms,
                    "build_s": t_build},
     }
     eng.end()

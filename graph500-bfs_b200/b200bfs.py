@@ -39,7 +39,7 @@ SYMBOLS = [
     "b200bfs_has_edge_all", "b200bfs_find_roots", "b200bfs_prepare", "b200bfs_run", "b200bfs_get_pred",
     "b200bfs_get_levels", "b200bfs_get_run_stats", "b200bfs_get_stream", "b200bfs_end",
     "b200bfs_auto_tune", "b200bfs_set_option", "b200bfs_get_level_stats",
-    "b200bfs_validate", "b200bfs_validate_pred", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select",
+    "b200bfs_validate", "b200bfs_validate_pred", "b200bfs_bfs_noalloc", "b200bfs_run_batch", "b200bfs_batch_select", "b200bfs_batch_root_levels",
     "b200bfs_server_start", "b200bfs_server_add_graph", "b200bfs_server_graph_info",
     "b200bfs_server_find_roots", "b200bfs_tune_engine",
     "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
@@ -190,6 +190,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
     L.b200bfs_tune_engine.argtypes = [H, vp, i32, i32, dbl, dbl, i32, P(TuneReport)]
     L.b200bfs_batch_select.argtypes = [H, i32]
+    L.b200bfs_batch_root_levels.argtypes = [H, ctypes.c_void_p]
     S = ctypes.c_void_p
     L.b200bfs_server_start.argtypes = [P(ServerConfig), P(S)]
     L.b200bfs_server_add_graph.argtypes = [S, i32, i32, u64, u64, i32, P(ctypes.c_int)]
@@ -355,6 +356,7 @@ class Engine:
     def run_batch(self, roots, edgefactor=16, alpha=BATCH_ALPHA, beta=DEFAULT_BETA):
         """One multi-source search from up to 64 roots; returns BatchStats."""
         r = np.ascontiguousarray(np.asarray(roots, dtype=np.int64))
+        self._batch_k = len(r)
         bs = BatchStats()
         self.check(self.L.b200bfs_run_batch(self.h, _ptr(r), len(r), edgefactor, alpha, beta,
                                             ctypes.byref(bs)))
@@ -368,6 +370,13 @@ class Engine:
         self.check(self.L.b200bfs_tune_engine(self.h, _ptr(r), len(r), edgefactor, alpha, beta,
                                               what, ctypes.byref(rep)))
         return rep
+
+    def batch_root_levels(self):
+        """AUTO_LEVEL of each root of the last batch (its deepest level + 1),
+        what b200bfs_run would report for that root alone."""
+        out = np.zeros(BATCH_MAX, dtype=np.int64)
+        self.check(self.L.b200bfs_batch_root_levels(self.h, _ptr(out)))
+        return out[: getattr(self, "_batch_k", BATCH_MAX)]
 
     def batch_select(self, index):
         """Makes root `index` of the last batch the current result (pred,

@@ -625,6 +625,17 @@ int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, in
   });
 }
 
+int b200bfs_batch_root_levels(b200bfs_handle* h, int64_t* auto_level) {
+  return guarded(h, [&](Engine& e) {
+    require(auto_level != nullptr, B200BFS_ERR_INVALID, "null output");
+    require(e.prepared && e.bs.allocated && e.bs.K > 0, B200BFS_ERR_STATE, "no batch has run");
+    for (int i = 0; i < e.bs.K; ++i) {
+      const long long L = e.bs.hctl->last_level[i];
+      auto_level[i] = L < 0 ? 0 : L + 1;
+    }
+  });
+}
+
 int b200bfs_batch_select(b200bfs_handle* h, int index) {
   return guarded(h, [&](Engine& e) {
     require(e.prepared && e.bs.allocated && e.bs.K > 0, B200BFS_ERR_STATE, "no batch has run");

@@ -610,6 +610,7 @@ __global__ void __launch_bounds__(kBatchMax) batch_control_kernel(
     c.prev_cnt[k] = n;
   }
   if (seeded & bit) c.prev_cnt[k] = 0;
+  if (act & bit) c.last_level[k] = L;
   __syncthreads();
   if (k == 0) {
     c.pending = pending & ~s_entered;
@@ -710,6 +711,7 @@ __global__ void batch_setup_kernel(BatchCtl* __restrict__ ctl, const BatchSetupA
     ctl->root_row[t] = row;
     ctl->root_lv[t] = t < a.K ? a.lv[t] : 0;
     ctl->prev_cnt[t] = 0;
+    ctl->last_level[t] = -1;
   }
   if (t == 0) {
     ctl->planes = a.planes;

@@ -63,6 +63,7 @@ struct BatchCtl {
   // per-root switch state (the reference rule, bfs.hpp:3413-3457, per root)
   unsigned long long bu_mask, growing, pending;
   long long prev_cnt[kBatchMax];
+  long long last_level[kBatchMax];  // deepest level at which root k found a vertex, -1 none
   BatchCounters c;
   BatchLevelRec hist[kBatchHist];
 };

@@ -348,6 +348,14 @@ int b200bfs_validate_pred(b200bfs_handle* h, int64_t root, const int64_t* pred, 
 int b200bfs_run_batch(b200bfs_handle* h, const int64_t* roots, int num_roots, int edgefactor,
                       double alpha, double beta, b200bfs_batch_stats* stats);
 
+/* auto_tuning_data[AUTO_LEVEL] of every root of the last batch, as
+ * b200bfs_run would leave it for that root alone: the first level at which
+ * the root's frontier is empty (its deepest level + 1; 0 for a root outside
+ * the searched graph).  The quantity find_roots_in_large_graph
+ * (main.cc:334-359) tests against REMOVE_ROOTS_LEVEL_THED, for all roots of
+ * one batch at once.  auto_level[num_roots] (host). */
+int b200bfs_batch_root_levels(b200bfs_handle* h, int64_t* auto_level);
+
 /* Makes root `index` of the last batch the engine's current result: pred is
  * rebuilt on the device from the batch's levels (parent = a neighbour one
  * level nearer the root, a valid BFS parent), so b200bfs_get_pred,

@@ -202,3 +202,22 @@ def test_batch_errors(engine, graphs):
     with pytest.raises(b200bfs.B200BfsError) as ex:
         engine.batch_select(2)
     assert ex.value.code == 1
+
+
+@pytest.mark.parametrize("scale,flags", [(16, 0), (20, 0), (16, 3), (20, 3)])
+def test_batch_root_levels_match_single_root(engine, scale, flags):
+    """b200bfs_batch_root_levels gives, for every root of a batch, the
+    AUTO_LEVEL slot b200bfs_run leaves for that root alone, so the re-pick
+    test of find_roots_in_large_graph (main.cc:334-359: pick again while a
+    root reaches <= 3 levels) can run as one batch.  Plain, and CoreBFS with
+    group reordering (roots climbing into the core)."""
+    engine.generate_graph(scale, 16, flags=flags)
+    engine.prepare(16)
+    for seed in range(4):
+        roots = engine.find_roots(64, seed, 0)
+        engine.run_batch(roots, 16, 0.0)
+        lv = engine.batch_root_levels()
+        single = np.array([engine.run(int(r), 16)[8] for r in roots])
+        assert np.array_equal(lv, single), (seed, lv, single)
+        assert (lv <= 3).any() == (single <= 3).any()
+    engine.end()
