@@ -418,7 +418,167 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
 // first[] array (one coalesced read for the warp), and loads its row offsets
 // only when that probe misses; the offset rounds then start at the second
 // neighbour.
+// The row search of the bottom-up forms for kWords bitmap words w[k] (w[k]
+// < 0: no word) whose current visited words are c[k]: lane l handles row
+// w[k] * 32 + l of each word, and the word's next value c[k] | found is
+// written to nxt.
 template <int kWords, bool kFirst>
+__device__ __forceinline__ void bu_rows(
+    const int64_t (&w)[kWords], const uint32_t (&c)[kWords], const uint32_t* __restrict__ cur,
+    uint32_t* __restrict__ nxt, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ col, const int32_t* __restrict__ first,
+    const int32_t* __restrict__ finv, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, int64_t* __restrict__ pred, int64_t level,
+    uint32_t& found_total, uint32_t& scanned) {
+  const int lane = lane_id();
+    // open row w[k] * 32 + lane: its next neighbour is col[b[k]] and
+  // rem[k] of them are left (a row has fewer than 2^31 neighbours)
+  int64_t b[kWords];
+  int32_t rem[kWords];
+  int32_t par[kWords];
+  // the parent is the row's first neighbour: its original id is then read
+  // from finv[] (a coalesced load) instead of gathered from inv[].  The
+  // 4-word form, which has registers to spare and fewer warps to hide
+  // latency with, loads it beside first[]; the 2-word forms at the end,
+  // for the rows whose first probe hit (fewer registers, no spills).
+  constexpr bool kEagerFinv = kWords >= 4;
+  bool pf[kWords];
+  int32_t fo[kEagerFinv ? kWords : 1];
+  if (kFirst) {
+    int32_t f[kWords];
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      par[k] = -1;
+      pf[k] = false;
+      b[k] = 0;
+      rem[k] = 0;
+      f[k] = -1;
+      if (kEagerFinv) fo[kEagerFinv ? k : 0] = -1;
+      if (((~c[k]) >> lane) & 1u) {
+        f[k] = __ldg(first + w[k] * 32 + lane);
+        if (kEagerFinv && finv) fo[kEagerFinv ? k : 0] = __ldg(finv + w[k] * 32 + lane);
+      }
+    }
+    uint32_t mf[kWords];
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) mf[k] = f[k] >= 0 ? __ldg(cur + (f[k] >> 5)) : 0u;
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      if (f[k] < 0) continue;
+      scanned += 1;
+      if ((mf[k] >> (f[k] & 31)) & 1u) {
+        par[k] = f[k];
+        pf[k] = true;
+      } else {
+        const int64_t v = w[k] * 32 + lane;
+        const int64_t rb = row_ptr[v];
+        b[k] = rb + 1;
+        rem[k] = (int32_t)(row_ptr[v + 1] - rb - 1);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      par[k] = -1;
+      pf[k] = false;
+      b[k] = 0;
+      rem[k] = 0;
+      if (((~c[k]) >> lane) & 1u) {
+        const int64_t v = w[k] * 32 + lane;
+        b[k] = row_ptr[v];
+        rem[k] = (int32_t)(row_ptr[v + 1] - b[k]);
+      }
+    }
+  }
+  // four rounds of two probes per vertex
+#pragma unroll
+  for (int round = 0; round < 4; ++round) {
+    int32_t u0[kWords], u1[kWords];
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      u0[k] = u1[k] = -1;
+      if (par[k] < 0 && rem[k] > 0) {
+        u0[k] = __ldg(col + b[k]);
+        if (rem[k] > 1) u1[k] = __ldg(col + b[k] + 1);
+        need = true;
+      }
+    }
+    if (!__any_sync(kFull, need)) break;
+    uint32_t m0[kWords], m1[kWords];
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      m0[k] = u0[k] >= 0 ? __ldg(cur + (u0[k] >> 5)) : 0u;
+      m1[k] = u1[k] >= 0 ? __ldg(cur + (u1[k] >> 5)) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+      if (u0[k] < 0) continue;
+      if ((m0[k] >> (u0[k] & 31)) & 1u) {
+        par[k] = u0[k];
+        scanned += 1;
+      } else if (u1[k] >= 0 && ((m1[k] >> (u1[k] & 31)) & 1u)) {
+        par[k] = u1[k];
+        scanned += 2;
+      } else {
+        const int32_t t = (u1[k] >= 0) ? 2 : 1;
+        scanned += t;
+        b[k] += t;
+        rem[k] -= t;
+      }
+    }
+  }
+  // cooperative sweep of the rows still unresolved
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) {
+    unsigned left = __ballot_sync(kFull, par[k] < 0 && rem[k] > 0);
+    while (left) {
+      const int l = __ffs(left) - 1;
+      left &= left - 1;
+      const int64_t jb = __shfl_sync(kFull, b[k], l);
+      const int64_t je = jb + __shfl_sync(kFull, rem[k], l);
+      int32_t p = -1;
+      for (int64_t j = jb; j < je; j += 32) {
+        const int64_t jj = j + lane;
+        int32_t u = 0;
+        bool hit = false;
+        if (jj < je) {
+          u = __ldg(col + jj);
+          hit = bit_test(cur, u);
+        }
+        const unsigned hm = __ballot_sync(kFull, hit);
+        if (hm) {
+          const int fl = __ffs(hm) - 1;
+          p = __shfl_sync(kFull, u, fl);
+          if (lane == l) scanned += (uint32_t)(j - jb + fl + 1);
+          break;
+        }
+      }
+      if (p < 0 && lane == l) scanned += (uint32_t)(je - jb);
+      if (lane == l) par[k] = p;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) {
+    const unsigned fm = __ballot_sync(kFull, par[k] >= 0);
+    if (lane == 0 && w[k] >= 0) {
+      nxt[w[k]] = c[k] | fm;
+      found_total += __popc(fm);
+    }
+    if (par[k] >= 0) {
+      const int64_t v = w[k] * 32 + lane;
+      int32_t po;
+      if (kEagerFinv && kFirst)
+        po = (pf[k] && fo[kEagerFinv ? k : 0] >= 0) ? fo[kEagerFinv ? k : 0]
+                                                   : __ldg(inv + par[k]);
+      else
+        po = (pf[k] && finv) ? __ldg(finv + v) : __ldg(inv + par[k]);
+      pred[pred_slot(pidx, v)] = pred_entry(po, level);
+    }
+  }
+}
+
+template <int kWords, bool kFirst, bool kSparse>
 __device__ __forceinline__ void bu_wide_body(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
@@ -428,150 +588,65 @@ __device__ __forceinline__ void bu_wide_body(
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long found_total = 0, scanned = 0;
-  for (int64_t w0 = gw * kWords; w0 < W; w0 += nwarps * kWords) {
-    uint32_t c[kWords];
-    bool all_full = true;
+  // per-lane counts (a lane scans far fewer than 2^32 entries), added to
+  // the 64-bit level counters once at the end
+  uint32_t found_total = 0, scanned = 0;
+  if (kSparse) {
+    // Few unvisited rows left (the last levels): a warp takes blocks of 32
+    // bitmap words, one per lane; full words are copied to nxt at once and
+    // only the words with unvisited rows go through the row search, kWords
+    // at a time.  A block costs one load per lane instead of 32 / kWords
+    // dependent word steps.
+    const int64_t nblk = (W + 31) >> 5;
+    for (int64_t blk = gw; blk < nblk; blk += nwarps) {
+      const int64_t wl = (blk << 5) + lane;
+      const uint32_t cl = wl < W ? cur[wl] : kFull;
+      if (cl == kFull && wl < W) nxt[wl] = kFull;
+      unsigned om = __ballot_sync(kFull, cl != kFull);
+      while (om) {
+        int64_t w[kWords];
+        uint32_t c[kWords];
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      c[k] = (w0 + k < W) ? cur[w0 + k] : kFull;
-      all_full &= (c[k] == kFull);
-    }
-    if (all_full) {
-      if (lane < kWords && w0 + lane < W) nxt[w0 + lane] = kFull;
-      continue;
-    }
-    int64_t b[kWords], e[kWords];
-    int32_t par[kWords];
-    // original id of the parent when it is the first neighbour (from finv,
-    // loaded with first[]); -1: looked up in inv[] at the end
-    int32_t po[kWords];
-    if (kFirst) {
-      int32_t f[kWords], fo[kWords];
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        par[k] = -1;
-        po[k] = -1;
-        b[k] = e[k] = 0;
-        f[k] = -1;
-        fo[k] = -1;
-        if (((~c[k]) >> lane) & 1u) {
-          f[k] = __ldg(first + (w0 + k) * 32 + lane);
-          if (finv) fo[k] = __ldg(finv + (w0 + k) * 32 + lane);
-        }
-      }
-      uint32_t mf[kWords];
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) mf[k] = f[k] >= 0 ? __ldg(cur + (f[k] >> 5)) : 0u;
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        if (f[k] < 0) continue;
-        scanned += 1;
-        if ((mf[k] >> (f[k] & 31)) & 1u) {
-          par[k] = f[k];
-          po[k] = fo[k];
-        } else {
-          const int64_t v = (w0 + k) * 32 + lane;
-          b[k] = row_ptr[v] + 1;
-          e[k] = row_ptr[v + 1];
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        par[k] = -1;
-        po[k] = -1;
-        b[k] = e[k] = 0;
-        if (((~c[k]) >> lane) & 1u) {
-          const int64_t v = (w0 + k) * 32 + lane;
-          b[k] = row_ptr[v];
-          e[k] = row_ptr[v + 1];
-        }
-      }
-    }
-    // four rounds of two probes per vertex
-#pragma unroll
-    for (int round = 0; round < 4; ++round) {
-      int32_t u0[kWords], u1[kWords];
-      bool need = false;
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        u0[k] = u1[k] = -1;
-        if (par[k] < 0 && b[k] < e[k]) {
-          u0[k] = __ldg(col + b[k]);
-          if (b[k] + 1 < e[k]) u1[k] = __ldg(col + b[k] + 1);
-          need = true;
-        }
-      }
-      if (!__any_sync(kFull, need)) break;
-      uint32_t m0[kWords], m1[kWords];
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        m0[k] = u0[k] >= 0 ? __ldg(cur + (u0[k] >> 5)) : 0u;
-        m1[k] = u1[k] >= 0 ? __ldg(cur + (u1[k] >> 5)) : 0u;
-      }
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        if (u0[k] < 0) continue;
-        if ((m0[k] >> (u0[k] & 31)) & 1u) {
-          par[k] = u0[k];
-          scanned += 1;
-        } else if (u1[k] >= 0 && ((m1[k] >> (u1[k] & 31)) & 1u)) {
-          par[k] = u1[k];
-          scanned += 2;
-        } else {
-          scanned += (u1[k] >= 0) ? 2 : 1;
-          b[k] = min(e[k], b[k] + 2);
-        }
-      }
-    }
-    // cooperative sweep of the rows still unresolved
-#pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      unsigned rem = __ballot_sync(kFull, par[k] < 0 && b[k] < e[k]);
-      while (rem) {
-        const int l = __ffs(rem) - 1;
-        rem &= rem - 1;
-        const int64_t jb = __shfl_sync(kFull, b[k], l), je = __shfl_sync(kFull, e[k], l);
-        int32_t p = -1;
-        for (int64_t j = jb; j < je; j += 32) {
-          const int64_t jj = j + lane;
-          int32_t u = 0;
-          bool hit = false;
-          if (jj < je) {
-            u = __ldg(col + jj);
-            hit = bit_test(cur, u);
-          }
-          const unsigned hm = __ballot_sync(kFull, hit);
-          if (hm) {
-            const int fl = __ffs(hm) - 1;
-            p = __shfl_sync(kFull, u, fl);
-            if (lane == l) scanned += (unsigned long long)(j - jb + fl + 1);
-            break;
+        for (int k = 0; k < kWords; ++k) {
+          w[k] = -1;
+          c[k] = kFull;
+          if (om) {
+            const int l = __ffs(om) - 1;
+            om &= om - 1;
+            w[k] = (blk << 5) + l;
+            c[k] = __shfl_sync(kFull, cl, l);
           }
         }
-        if (p < 0 && lane == l) scanned += (unsigned long long)(je - jb);
-        if (lane == l) par[k] = p;
+        bu_rows<kWords, kFirst>(w, c, cur, nxt, row_ptr, col, first, finv, inv, pidx, pred,
+                                level, found_total, scanned);
       }
     }
+  } else {
+    // kWords consecutive words per warp step, strided over the warps
+    for (int64_t w0 = gw * kWords; w0 < W; w0 += nwarps * kWords) {
+      int64_t w[kWords];
+      uint32_t c[kWords];
+      bool all_full = true;
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      const unsigned fm = __ballot_sync(kFull, par[k] >= 0);
-      if (lane == 0 && w0 + k < W) {
-        nxt[w0 + k] = c[k] | fm;
-        found_total += __popc(fm);
+      for (int k = 0; k < kWords; ++k) {
+        w[k] = w0 + k < W ? w0 + k : -1;
+        c[k] = w[k] >= 0 ? cur[w0 + k] : kFull;
+        all_full &= (c[k] == kFull);
       }
-      if (par[k] >= 0) {
-        const int64_t v = (w0 + k) * 32 + lane;
-        pred[pred_slot(pidx, v)] = pred_entry(po[k] >= 0 ? po[k] : __ldg(inv + par[k]), level);
+      if (all_full) {
+        if (lane < kWords && w0 + lane < W) nxt[w0 + lane] = kFull;
+        continue;
       }
+      bu_rows<kWords, kFirst>(w, c, cur, nxt, row_ptr, col, first, finv, inv, pidx, pred, level,
+                              found_total, scanned);
     }
   }
+  unsigned long long sc = scanned;
 #pragma unroll
-  for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(kFull, scanned, o);
+  for (int o = 16; o; o >>= 1) sc += __shfl_xor_sync(kFull, sc, o);
   if (lane == 0) {
-    if (found_total) atomicAdd(&ctr->nq, found_total);
-    if (scanned) atomicAdd(&ctr->scanned, scanned);
+    if (found_total) atomicAdd(&ctr->nq, (unsigned long long)found_total);
+    if (sc) atomicAdd(&ctr->scanned, sc);
   }
 }
 
@@ -1079,7 +1154,7 @@ __global__ void __launch_bounds__(256) td_expand_kernel(
   td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
-template <int kWords, int kMinBlocks, bool kFirst>
+template <int kWords, int kMinBlocks, bool kFirst, bool kSparse = false>
 __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
@@ -1087,8 +1162,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
     int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr,
     BfsState::Published* pub, unsigned long long seq) {
-  bu_wide_body<kWords, kFirst>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred, level,
-                               ctr);
+  bu_wide_body<kWords, kFirst, kSparse>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred,
+                                        level, ctr);
   publish_if_last(ctr, pub, seq);
 }
 
@@ -1264,7 +1339,8 @@ __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
     int64_t* __restrict__ pred, Counters* __restrict__ ctr) {
   if (c->done || c->forward) return;
   const int cur = c->cur;
-  bu_wide_body<4, kFirst>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, finv, inv, pidx,
+  bu_wide_body<4, kFirst, false>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, finv, inv,
+                                 pidx,
                           pred,
                           c->level, ctr);
 }
@@ -1720,8 +1796,9 @@ static Counters wait_level(BfsState& st, cudaStream_t s) {
 void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t root,
                   int64_t root_level, int edgefactor, double alpha, double beta, int64_t* at,
                   const RunOptions& opt, b200bfs_run_stats* stats) {
-  // the device-driven loop has top-down forms 1, 3, 4 and 5
-  if (opt.single_graph && opt.bu_kernel == 4 && opt.td_kernel != 2 && opt.td_kernel <= 5) {
+  // the device-driven loop has top-down forms 1, 3, 4 and 5 and its own
+  // bottom-up form (four words per warp step, as form 4)
+  if (opt.single_graph && opt.td_kernel != 2 && opt.td_kernel <= 5) {
     run_bfs_core_graph(g, st, s, sms, root, root_level, edgefactor, alpha, beta, at, opt, stats);
     return;
   }
@@ -1822,11 +1899,23 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
         kernel<<<bu_grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.inv,
                                      pidx, out, level, st.ctr, st.dpub, st.pub_seq + 1);
       };
-      if (opt.bu_kernel == 2)
+      // the last levels, with few unvisited rows left, skip full bitmap words
+      // 32 at a time (fewer than one unvisited row per four words)
+      const bool sparse = opt.bu_sparse && 4 * (st.R - visited) < st.W;
+      if (opt.bu_kernel == 2 && sparse)
+        launch_wide(first ? bu_wide_kernel<2, 8, true, true> : bu_wide_kernel<2, 8, false, true>,
+                    bu_wide_grid);
+      else if (opt.bu_kernel == 2)
         launch_wide(first ? bu_wide_kernel<2, 8, true> : bu_wide_kernel<2, 8, false>,
                     bu_wide_grid);
+      else if (opt.bu_kernel == 3 && sparse)
+        launch_wide(first ? bu_wide_kernel<2, 6, true, true> : bu_wide_kernel<2, 6, false, true>,
+                    sms * 6);
       else if (opt.bu_kernel == 3)
         launch_wide(first ? bu_wide_kernel<2, 6, true> : bu_wide_kernel<2, 6, false>, sms * 6);
+      else if (opt.bu_kernel == 4 && sparse)
+        launch_wide(first ? bu_wide_kernel<4, 4, true, true> : bu_wide_kernel<4, 4, false, true>,
+                    sms * 4);
       else if (opt.bu_kernel == 4)
         launch_wide(first ? bu_wide_kernel<4, 4, true> : bu_wide_kernel<4, 4, false>, sms * 4);
       else if (opt.bu_probe <= 4)

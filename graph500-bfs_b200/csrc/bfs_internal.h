@@ -106,8 +106,10 @@ struct BfsState {
 struct RunOptions {
   // Bottom-up form.  1: bu_kernel (one word per warp step); 2, 3, 4:
   // bu_wide_kernel with 2 words at 8 or 6 resident CTAs per SM, or 4 words
-  // at 4 per SM.  Form 4 is the fastest measured at SCALE 24 and 28.
-  int bu_kernel = 4;
+  // at 4 per SM.  Form 2 is the fastest measured at SCALE 28 (2.57 against
+  // 2.69 ms per search for forms 3 and 4 on the headline graph) and within
+  // 1 % of the best (form 3) at SCALE 24.
+  int bu_kernel = 2;
   // Top-down form.  1: td_expand_kernel, 2: td_wide_kernel, 3: td_chunk_kernel,
   // 4: form 5 while the frontier grows, form 3 after the switch back from
   // bottom-up (measured best at SCALE 24 and 28), 5: td_expand_kernel with a
@@ -117,6 +119,10 @@ struct RunOptions {
   int td_kernel = 4;
   int bu_probe = 8;         // bu_kernel: neighbours each lane probes before the warp sweep
   int bu_first = 1;         // bottom-up form 4: probe the dense first-neighbour array first
+  // bottom-up forms 2-4 on levels with fewer unvisited rows than a quarter of
+  // the bitmap words: skip full words 32 at a time (1) or step through every
+  // word (0)
+  int bu_sparse = 1;
   int td_unroll = 1;        // td form 5: 32-entry steps per lane handled together (1, 2, 4)
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
   // pred output.  1: the level kernels write a row-order buffer and one

@@ -551,6 +551,9 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "batch_alpha") {
       require(value >= 1 && value <= 1000000, B200BFS_ERR_INVALID, "batch_alpha must be 1..1e6");
       e.opt.batch_alpha = (double)value;
+    } else if (n == "bu_sparse") {
+      require(value == 0 || value == 1, B200BFS_ERR_INVALID, "bu_sparse must be 0 or 1");
+      e.opt.bu_sparse = (int)value;
     } else if (n == "force_direction") {
       require(value >= 0 && value <= 2, B200BFS_ERR_INVALID, "force_direction must be 0..2");
       e.opt.force_direction = (int)value;

@@ -283,7 +283,9 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * kernel form), "td_kernel" (1..7, top-down kernel form; 4 and 7 pick per
  * level), "bu_probe" (1..64, neighbours probed per lane by bottom-up form
  * 1), "bu_first" (1: bottom-up forms 2-4 probe the first neighbour from a
- * dense per-row array first, the default), "td_unroll" (1, 2 or 4: 32-entry
+ * dense per-row array first, the default), "bu_sparse" (1: on levels with
+ * few unvisited rows bottom-up forms 2-4 skip full bitmap words 32 at a time,
+ * the default; 0: every word steps through the row search), "td_unroll" (1, 2 or 4: 32-entry
  * steps a lane of top-down form 5 handles together), "pred_assemble" (1:
  * the levels write a row-order buffer and one pass over the original ids
  * writes pred, the default; after a search of this kind the pass leaves out

@@ -321,7 +321,7 @@ def test_kernel_forms_agree(engine, oracle_graphs, bu, td, first):
         _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 3))
         _check_search(engine, edges, g, O.find_roots(g.has_edge(), 1 << 18, 2), alpha=1e-9)
     finally:
-        engine.set_option("bu_kernel", 4)
+        engine.set_option("bu_kernel", 2)
         engine.set_option("td_kernel", 4)
         engine.set_option("bu_first", 1)
         engine.end()
@@ -355,7 +355,7 @@ def test_engine_tuner_keeps_results_exact(engine, oracle_graphs):
         assert rep.beta in [14.0 * f for f in (0.5, 0.7, 1.0, 1.4, 2.0)]
         _check_search(engine, edges, g, roots[:3], alpha=rep.alpha, beta=rep.beta)
     finally:
-        engine.set_option("bu_kernel", 4)
+        engine.set_option("bu_kernel", 2)
         engine.set_option("td_kernel", 4)
         engine.set_option("batch_alpha", 30)
         engine.end()
@@ -468,3 +468,28 @@ def test_find_roots_matches_oracle(engine, oracle_graphs, scale, flags):
         dev = engine.find_roots(16, r1, r2)
         ref = O.find_roots(g.has_edge(), 1 << scale, 16, r1, r2)
         assert np.array_equal(dev, ref), (r1, r2)
+
+
+@pytest.mark.parametrize("bu,sparse", [(2, 0), (2, 1), (3, 1), (4, 1), (4, 0)])
+def test_bottom_up_sparse_levels_agree(engine, oracle_graphs, bu, sparse):
+    """Bottom-up forms with (bu_sparse 1) and without the skip of full
+    bitmap words on levels with few unvisited rows; every level after the
+    first runs bottom-up (force_direction 2), so the last levels take the
+    sparse path."""
+    edges, g = oracle_graphs(18)
+    engine.generate_graph(18, 16)
+    engine.set_option("bu_kernel", bu)
+    engine.set_option("bu_sparse", sparse)
+    engine.set_option("force_direction", 2)
+    engine.prepare(16)
+    try:
+        for r in O.find_roots(g.has_edge(), 1 << 18, 3):
+            engine.run(int(r), 16)
+            assert np.array_equal(engine.get_levels()[: g.nverts], g.levels(int(r)))
+            err, cnt = O.validate(edges, 1 << 18, engine.get_pred()[: g.nverts], int(r))
+            assert err == 0
+    finally:
+        engine.set_option("bu_kernel", 2)
+        engine.set_option("bu_sparse", 1)
+        engine.set_option("force_direction", 0)
+        engine.end()
