@@ -2,7 +2,10 @@
 //
 // The reference runs one root per BfsBase::run_bfs call (main.cc:610-640).
 // Here up to 64 roots share one traversal.  State per searched row v:
-//   seen[v]        uint64, bit k set once root k has reached v;
+//   seen[2v]       uint64, bit k set once root k has reached v; seen[2v + 1]
+//                  holds the bits the top-down push found for v in the current
+//                  level until the merge pass moves them (same 16 bytes, so a
+//                  push's probe and OR touch one sector);
 //   planes[L][v]   uint64, bit k set iff level_k(v) == L (the bit-sliced
 //                  level array of the batch; it is also the frontier of
 //                  level L).
@@ -276,11 +279,12 @@ __global__ void __launch_bounds__(kQThreads) batch_queue_write_kernel(
 
 // Top-down push for the roots in td_mask: edge-balanced over the queue rows
 // (each warp takes kBTile adjacency entries of the concatenated rows).  For
-// an edge (u, v) the bits m = planes[L-1][u] & td_mask not in seen[v] are
-// ORed (non-returning) into planes[L][v] and seen[v], and v is marked in the
-// touched-row bitmap.  seen[v] may be stale for bits set during this level;
-// those bits are new in level L all the same, so planes[L] still gets exactly
-// the (root, vertex) pairs first reached at level L.  Runs after the
+// an edge (u, v) the bits m = planes[L-1][u] & td_mask not yet in seen[2v]
+// nor in this level's new bits seen[2v + 1] are ORed (non-returning) into
+// seen[2v + 1], and v is marked in the touched-row bitmap; batch_merge_kernel
+// then moves the new bits into planes[L] and seen.  Both words of v are in
+// one 16-byte pair, so the probe and the OR touch one sector.  A stale pair
+// (bits set during the level) only costs a redundant OR.  Runs after the
 // bottom-up sweep of the level, which only writes bottom-up roots' bits.
 __global__ void __launch_bounds__(256) batch_td_kernel(
     BatchCtl* __restrict__ ctl, const int32_t* __restrict__ queue,
@@ -292,7 +296,6 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
   const long long L = ctl->level;
   const unsigned long long T = ctl->td_mask;
   const unsigned long long* __restrict__ prev = plane_ptr(ctl, L - 1);
-  unsigned long long* cur = plane_ptr(ctl, L);
   unsigned long long* seen = ctl->seen;
   uint32_t* rb = rowbits_of(ctl, L);
   const int64_t total = qdeg[qsize];
@@ -321,12 +324,11 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
         f = prev[src] & T;
       }
       const int32_t u = __ldg(col + rbeg + (e - seg_lo));
-      // L2 read: seen changes during the kernel; a stale value only costs
-      // redundant ORs
-      const unsigned long long m = f & ~__ldcg(seen + u);
+      // L2 read of the pair: it changes during the kernel
+      const ulonglong2 x = __ldcg(reinterpret_cast<const ulonglong2*>(seen) + u);
+      const unsigned long long m = f & ~(x.x | x.y);
       if (m) {
-        atomicOr(seen + u, m);
-        atomicOr(cur + u, m);
+        atomicOr(seen + 2 * (int64_t)u + 1, m);
         // the bitmap is L2-resident; most rows are marked by an earlier
         // edge, and a read costs less than an atomic
         const uint32_t bit = 1u << (u & 31);
@@ -337,6 +339,42 @@ __global__ void __launch_bounds__(256) batch_td_kernel(
   }
   found = warp_or64(found);
   if (lane == 0 && found) atomicOr(&ctl->c.active, found);
+}
+
+// After the top-down push: for every row of the level's touched-row bitmap,
+// the bits the push left in seen[2v + 1] are ORed into planes[L][v] (which
+// may hold the bottom-up sweep's bits of other roots) and seen[2v], and
+// seen[2v + 1] is cleared.  A warp reads 32 bitmap words and then handles
+// the 32 rows of each marked word together, one row per lane.
+__global__ void __launch_bounds__(256) batch_merge_kernel(BatchCtl* __restrict__ ctl) {
+  if (!ctl->has_td) return;
+  const long long L = ctl->level;
+  const int64_t R = ctl->R;
+  const int64_t W = (R + 31) >> 5;
+  const uint32_t* __restrict__ rb = rowbits_of(ctl, L);
+  unsigned long long* __restrict__ cur = plane_ptr(ctl, L);
+  ulonglong2* __restrict__ pair = reinterpret_cast<ulonglong2*>(ctl->seen);
+  const int lane = lane_id();
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = gw * 32; base < W; base += nwarps * 32) {
+    const int64_t w = base + lane;
+    const uint32_t bits = w < W ? __ldcg(rb + w) : 0u;
+    unsigned marked = __ballot_sync(kFull, bits != 0);
+    while (marked) {
+      const int l = __ffs(marked) - 1;
+      marked &= marked - 1;
+      const uint32_t word = __shfl_sync(kFull, bits, l);
+      const int64_t v = (base + l) * 32 + lane;
+      if (v < R && ((word >> lane) & 1u)) {
+        const ulonglong2 x = pair[v];
+        if (x.y) {
+          cur[v] |= x.y;
+          pair[v] = make_ulonglong2(x.x | x.y, 0ull);
+        }
+      }
+    }
+  }
 }
 
 // Bottom-up pull for the roots in bu_mask_active.  A warp owns 32
@@ -389,7 +427,7 @@ __global__ void __launch_bounds__(256, 5) batch_bu_kernel(BatchCtl* __restrict__
   uint32_t d_next = 0;
   if (gw < nchunks) {
     const int64_t v0 = gw * 32 + lane;
-    s_next = v0 < R ? seen[v0] : ~0ull;
+    s_next = v0 < R ? seen[2 * v0] : ~0ull;
     d_next = rb[gw];
   }
   for (int64_t ch = gw; ch < nchunks; ch += nwarps) {
@@ -399,7 +437,7 @@ __global__ void __launch_bounds__(256, 5) batch_bu_kernel(BatchCtl* __restrict__
     const unsigned long long s = s_next;
     if (ch + nwarps < nchunks) {
       const int64_t vn = v + nwarps * 32;
-      s_next = vn < R ? seen[vn] : ~0ull;
+      s_next = vn < R ? seen[2 * vn] : ~0ull;
       d_next = rb[ch + nwarps];
     }
     const unsigned long long U = ~s & Bm;
@@ -470,7 +508,7 @@ __global__ void __launch_bounds__(256, 5) batch_bu_kernel(BatchCtl* __restrict__
     const unsigned hit = __ballot_sync(kFull, n != 0);
     // whole 256-byte blocks: partial sector writes cost DRAM reads
     if (valid && (hit || dirty)) cur[v] = n;
-    if (valid && hit) seen[v] = s | n;
+    if (valid && hit) seen[2 * v] = s | n;
     if (lane == 0 && (hit || dirty)) rb[ch] = hit;
     found |= n;
   }
@@ -586,7 +624,7 @@ __global__ void __launch_bounds__(kBatchMax) batch_control_kernel(
     const int r = c.root_row[k];
     if (r >= 0) {
       atomicOr(plane_ptr(ctl, L) + r, bit);
-      atomicOr(c.seen + r, bit);
+      atomicOr(c.seen + 2 * (int64_t)r, bit);
       atomicOr(rowbits_of(ctl, L) + (r >> 5), 1u << (r & 31));
       atomicOr(&s_seeded, bit);
     }
@@ -690,7 +728,7 @@ __global__ void batch_zero_kernel(const BatchSetupArg* __restrict__ a) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool full = a->full_clear != 0;
-  zero_u64(seen, n, t0, stride);
+  zero_u64(seen, 2 * n, t0, stride);
   if (full) zero_u64(p0, n, t0, stride);
   if (!full && t0 < a->nclear) p0[a->clear[t0]] = 0ull;
   for (int64_t i = t0; i < ((n + 31) >> 5); i += stride) rb[i] = 0u;
@@ -968,7 +1006,8 @@ void batch_allocate(DeviceArena& arena, const Graph& g, BatchState& bs) {
   bs.R = g.csr.nrows;
   const int64_t W = (bs.R + 31) / 32;
   bs.nblk = (W + kQThreads - 1) / kQThreads;
-  bs.seen = arena_alloc<unsigned long long>(arena, bs.R, "batch seen masks");
+  // (seen, new bits of the level) pairs, see batch_td_kernel
+  bs.seen = arena_alloc<unsigned long long>(arena, 2 * bs.R, "batch seen masks");
   bs.wstride = (W + 4) & ~(int64_t)3;
   bs.queue = arena_alloc<int32_t>(arena, bs.R + 1, "batch frontier queue");
   bs.qdeg = arena_alloc<int64_t>(arena, bs.R + 2, "batch frontier degree prefix");
@@ -1070,11 +1109,12 @@ void launch_level(const Graph& g, BatchState& bs, cudaStream_t s, int sms,
   if (ev) check_cuda(cudaEventRecord(ev[2], s), "event");
   batch_td_kernel<<<sms * blocks_per_sm(batch_td_kernel, B), B, 0, s>>>(bs.ctl, bs.queue, bs.qdeg,
                                                                       c.row_ptr, c.col);
+  batch_merge_kernel<<<sms * blocks_per_sm(batch_merge_kernel, B), B, 0, s>>>(bs.ctl);
   if (ev) check_cuda(cudaEventRecord(ev[3], s), "event");
   batch_stats_kernel<<<sms * blocks_per_sm(batch_stats_kernel, B), B, 0, s>>>(bs.ctl, c.mdeg);
   batch_control_kernel<<<1, kBatchMax, 0, s>>>(bs.ctl, c.mdeg, cond, use_cond);
 }
-constexpr int kLevelLaunches = 8;
+constexpr int kLevelLaunches = 9;
 
 void launch_prologue(const Graph& g, BatchState& bs, cudaStream_t s, int sms) {
   batch_zero_kernel<<<grid_for(bs.R, 256, sms, 8), 256, 0, s>>>(
