@@ -219,7 +219,33 @@ __global__ void pred_map_kernel(const int32_t* __restrict__ rank, const int32_t*
 // kUnroll: 32-entry steps handled together by a lane (all neighbour ids of
 // the steps loaded, then all visited probes, then the claims), so more
 // independent loads are in flight.
-template <bool kWarpSearch, int kUnroll>
+// How a top-down entry probes and claims its neighbour u (kClaim bits).
+// Bit 0: the visited word is read from L2 (ld.global.cg) instead of through
+// L1, whose lines do not see the ORs other warps make during the level.
+// Bit 1: an unvisited u is claimed with an atomic OR that returns the old
+// word, and only the warp lane that set the bit writes u's pred entry;
+// without it every entry that saw u unvisited writes (a redundant but valid
+// parent) and ORs without a return.
+template <int kClaim>
+__device__ __forceinline__ uint32_t td_probe(const uint32_t* vis, int32_t u) {
+  return (kClaim & 1) ? __ldcg(vis + (u >> 5)) : vis[u >> 5];
+}
+
+template <int kClaim>
+__device__ __forceinline__ void td_claim_as(int32_t u, uint32_t word, int64_t entry,
+                                            const int32_t* __restrict__ pidx, uint32_t* vis,
+                                            int64_t* __restrict__ pred) {
+  const uint32_t bit = 1u << (u & 31);
+  if ((word & bit) != 0) return;
+  if (kClaim & 2) {
+    if ((atomicOr(vis + (u >> 5), bit) & bit) == 0) pred[pred_slot(pidx, u)] = entry;
+  } else {
+    pred[pred_slot(pidx, u)] = entry;
+    red_or(vis + (u >> 5), bit);
+  }
+}
+
+template <bool kWarpSearch, int kUnroll, int kClaim = 0>
 __device__ __forceinline__ void td_expand_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -278,15 +304,14 @@ __device__ __forceinline__ void td_expand_body(
       // causes a redundant (still valid) claim
       uint32_t words[kUnroll];
 #pragma unroll
-      for (int j = 0; j < kUnroll; ++j) words[j] = us[j] >= 0 ? vis[us[j] >> 5] : kFull;
+      for (int j = 0; j < kUnroll; ++j) words[j] = us[j] >= 0 ? td_probe<kClaim>(vis, us[j]) : kFull;
 #pragma unroll
       for (int j = 0; j < kUnroll; ++j) {
         if (us[j] < 0) continue;
         const uint32_t bit = 1u << (us[j] & 31);
-        if ((words[j] & bit) == 0) {
-          pred[pred_slot(pidx, us[j])] = pred_entry(__ldg(inv + srcs[j]), level);
-          red_or(vis + (us[j] >> 5), bit);
-        }
+        if ((words[j] & bit) == 0)
+          td_claim_as<kClaim>(us[j], words[j], pred_entry(__ldg(inv + srcs[j]), level), pidx, vis,
+                              pred);
       }
     }
   }
@@ -414,60 +439,62 @@ __global__ void __launch_bounds__(256) bu_kernel(const uint32_t* __restrict__ cu
 // probes, back to back: kWords * 2 independent loads are in flight per lane
 // instead of one dependent chain.  Rows unresolved after 8 probes are swept
 // by the whole warp as in bu_kernel.
-// kFirst: each open row first probes its first neighbour from the dense
-// first[] array (one coalesced read for the warp), and loads its row offsets
-// only when that probe misses; the offset rounds then start at the second
-// neighbour.
+// kFirst: each open row first probes its first neighbour, read from the
+// dense fpair[] array together with that neighbour's original id (one
+// coalesced 8-byte read per row), and loads its row offsets only when that
+// probe misses; the offset rounds then start at the second neighbour.  A
+// parent found by the first probe has its pred entry's id at hand: no
+// second load, no gather into inv[].
+// kSpec (with kFirst): the fpair[] loads are issued for every row of the
+// words, beside the loads of the words themselves, and the visited rows'
+// entries are dropped afterwards: one round trip fewer per step, for the
+// levels where most rows are still unvisited.
 // The row search of the bottom-up forms for kWords bitmap words w[k] (w[k]
 // < 0: no word) whose current visited words are c[k]: lane l handles row
 // w[k] * 32 + l of each word, and the word's next value c[k] | found is
 // written to nxt.
-template <int kWords, bool kFirst>
+template <int kWords, bool kFirst, bool kSpec = false>
 __device__ __forceinline__ void bu_rows(
     const int64_t (&w)[kWords], const uint32_t (&c)[kWords], const uint32_t* __restrict__ cur,
     uint32_t* __restrict__ nxt, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ first,
-    const int32_t* __restrict__ finv, const int32_t* __restrict__ inv,
-    const int32_t* __restrict__ pidx, int64_t* __restrict__ pred, int64_t level,
-    uint32_t& found_total, uint32_t& scanned) {
+    const int32_t* __restrict__ col, const int2* __restrict__ fpair,
+    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
+    int64_t* __restrict__ pred, int64_t level, uint32_t& found_total, uint32_t& scanned) {
   const int lane = lane_id();
-    // open row w[k] * 32 + lane: its next neighbour is col[b[k]] and
+  // open row w[k] * 32 + lane: its next neighbour is col[b[k]] and
   // rem[k] of them are left (a row has fewer than 2^31 neighbours)
   int64_t b[kWords];
   int32_t rem[kWords];
+  // par[k]: the parent's row id, or with pf[k] (found by the first probe)
+  // already its original id
   int32_t par[kWords];
-  // the parent is the row's first neighbour: its original id is then read
-  // from finv[] (a coalesced load) instead of gathered from inv[].  The
-  // 4-word form, which has registers to spare and fewer warps to hide
-  // latency with, loads it beside first[]; the 2-word forms at the end,
-  // for the rows whose first probe hit (fewer registers, no spills).
-  constexpr bool kEagerFinv = kWords >= 4;
   bool pf[kWords];
-  int32_t fo[kEagerFinv ? kWords : 1];
   if (kFirst) {
-    int32_t f[kWords];
+    int2 f[kWords];
 #pragma unroll
     for (int k = 0; k < kWords; ++k) {
       par[k] = -1;
       pf[k] = false;
       b[k] = 0;
       rem[k] = 0;
-      f[k] = -1;
-      if (kEagerFinv) fo[kEagerFinv ? k : 0] = -1;
-      if (((~c[k]) >> lane) & 1u) {
-        f[k] = __ldg(first + w[k] * 32 + lane);
-        if (kEagerFinv && finv) fo[kEagerFinv ? k : 0] = __ldg(finv + w[k] * 32 + lane);
-      }
+      f[k] = make_int2(-1, -1);
+      if (kSpec ? w[k] >= 0 : (((~c[k]) >> lane) & 1u) != 0)
+        f[k] = __ldg(fpair + w[k] * 32 + lane);
+    }
+    if (kSpec) {
+#pragma unroll
+      for (int k = 0; k < kWords; ++k)
+        if (((c[k] >> lane) & 1u) != 0) f[k].x = -1;
     }
     uint32_t mf[kWords];
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) mf[k] = f[k] >= 0 ? __ldg(cur + (f[k] >> 5)) : 0u;
+    for (int k = 0; k < kWords; ++k) mf[k] = f[k].x >= 0 ? __ldg(cur + (f[k].x >> 5)) : 0u;
 #pragma unroll
     for (int k = 0; k < kWords; ++k) {
-      if (f[k] < 0) continue;
+      if (f[k].x < 0) continue;
       scanned += 1;
-      if ((mf[k] >> (f[k] & 31)) & 1u) {
-        par[k] = f[k];
+      if ((mf[k] >> (f[k].x & 31)) & 1u) {
+        par[k] = f[k].y;
         pf[k] = true;
       } else {
         const int64_t v = w[k] * 32 + lane;
@@ -567,24 +594,19 @@ __device__ __forceinline__ void bu_rows(
     }
     if (par[k] >= 0) {
       const int64_t v = w[k] * 32 + lane;
-      int32_t po;
-      if (kEagerFinv && kFirst)
-        po = (pf[k] && fo[kEagerFinv ? k : 0] >= 0) ? fo[kEagerFinv ? k : 0]
-                                                   : __ldg(inv + par[k]);
-      else
-        po = (pf[k] && finv) ? __ldg(finv + v) : __ldg(inv + par[k]);
+      const int32_t po = pf[k] ? par[k] : __ldg(inv + par[k]);
       pred[pred_slot(pidx, v)] = pred_entry(po, level);
     }
   }
 }
 
-template <int kWords, bool kFirst, bool kSparse>
+template <int kWords, bool kFirst, bool kSparse, bool kSpec = false>
 __device__ __forceinline__ void bu_wide_body(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ first, const int32_t* __restrict__ finv,
-    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
-    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr) {
+    const int2* __restrict__ fpair, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, int64_t* __restrict__ pred, int64_t level,
+    Counters* __restrict__ ctr) {
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -617,7 +639,7 @@ __device__ __forceinline__ void bu_wide_body(
             c[k] = __shfl_sync(kFull, cl, l);
           }
         }
-        bu_rows<kWords, kFirst>(w, c, cur, nxt, row_ptr, col, first, finv, inv, pidx, pred,
+        bu_rows<kWords, kFirst>(w, c, cur, nxt, row_ptr, col, fpair, inv, pidx, pred,
                                 level, found_total, scanned);
       }
     }
@@ -633,11 +655,12 @@ __device__ __forceinline__ void bu_wide_body(
         c[k] = w[k] >= 0 ? cur[w0 + k] : kFull;
         all_full &= (c[k] == kFull);
       }
-      if (all_full) {
+      // (kSpec issues the row loads before the words arrive: no early exit)
+      if (!kSpec && all_full) {
         if (lane < kWords && w0 + lane < W) nxt[w0 + lane] = kFull;
         continue;
       }
-      bu_rows<kWords, kFirst>(w, c, cur, nxt, row_ptr, col, first, finv, inv, pidx, pred, level,
+      bu_rows<kWords, kFirst, kSpec>(w, c, cur, nxt, row_ptr, col, fpair, inv, pidx, pred, level,
                               found_total, scanned);
     }
   }
@@ -828,16 +851,7 @@ __device__ __forceinline__ void td_chunk_body(
 // for the next step.
 constexpr int kVecTile = 1024;  // entries per warp tile: 8 steps of 128
 
-__device__ __forceinline__ void td_claim(int32_t u, uint32_t word, int64_t entry,
-                                         const int32_t* __restrict__ pidx, uint32_t* vis,
-                                         int64_t* __restrict__ pred) {
-  const uint32_t bit = 1u << (u & 31);
-  if ((word & bit) == 0) {
-    pred[pred_slot(pidx, u)] = entry;
-    red_or(vis + (u >> 5), bit);
-  }
-}
-
+template <int kClaim = 0>
 __device__ __forceinline__ void td_vec_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -887,12 +901,12 @@ __device__ __forceinline__ void td_vec_body(
         }
         // plain loads: vis is being updated by this kernel; a stale word
         // only causes a redundant (still valid) claim
-        const uint32_t w0 = vis[u0 >> 5], w1 = vis[u1 >> 5], w2 = vis[u2 >> 5],
-                       w3 = vis[u3 >> 5];
-        td_claim(u0, w0, entry, pidx, vis, pred);
-        td_claim(u1, w1, entry, pidx, vis, pred);
-        td_claim(u2, w2, entry, pidx, vis, pred);
-        td_claim(u3, w3, entry, pidx, vis, pred);
+        const uint32_t w0 = td_probe<kClaim>(vis, u0), w1 = td_probe<kClaim>(vis, u1),
+                       w2 = td_probe<kClaim>(vis, u2), w3 = td_probe<kClaim>(vis, u3);
+        td_claim_as<kClaim>(u0, w0, entry, pidx, vis, pred);
+        td_claim_as<kClaim>(u1, w1, entry, pidx, vis, pred);
+        td_claim_as<kClaim>(u2, w2, entry, pidx, vis, pred);
+        td_claim_as<kClaim>(u3, w3, entry, pidx, vis, pred);
         continue;
       }
       // the step crosses a row boundary: per-lane walk over 32-entry sub-steps
@@ -911,7 +925,8 @@ __device__ __forceinline__ void td_vec_body(
             l_rb = row_ptr[l_src];
           }
           const int32_t u = __ldg(col + l_rb + (e - l_lo));
-          td_claim(u, vis[u >> 5], pred_entry(__ldg(inv + l_src), level), pidx, vis, pred);
+          td_claim_as<kClaim>(u, td_probe<kClaim>(vis, u), pred_entry(__ldg(inv + l_src), level),
+                              pidx, vis, pred);
         }
       }
       // lane 31 walked furthest (to the row of entry e0 + 127, when the tile
@@ -1144,36 +1159,37 @@ __device__ __forceinline__ void frontier_write_body(
 
 // Kernels of the host-driven level loop: thin wrappers around the bodies
 // above, which the device-driven loop (below) shares.
-template <bool kWarpSearch, int kUnroll>
+template <bool kWarpSearch, int kUnroll, int kClaim = 0>
 __global__ void __launch_bounds__(256) td_expand_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
     const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
+  td_expand_body<kWarpSearch, kUnroll, kClaim>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred,
+                                               level);
 }
 
-template <int kWords, int kMinBlocks, bool kFirst, bool kSparse = false>
+template <int kWords, int kMinBlocks, bool kFirst, bool kSparse = false, bool kSpec = false>
 __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
     const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int64_t W,
     const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-    const int32_t* __restrict__ first, const int32_t* __restrict__ finv,
-    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
-    int64_t* __restrict__ pred, int64_t level, Counters* __restrict__ ctr,
-    BfsState::Published* pub, unsigned long long seq) {
-  bu_wide_body<kWords, kFirst, kSparse>(cur, nxt, W, row_ptr, col, first, finv, inv, pidx, pred,
-                                        level, ctr);
+    const int2* __restrict__ fpair, const int32_t* __restrict__ inv,
+    const int32_t* __restrict__ pidx, int64_t* __restrict__ pred, int64_t level,
+    Counters* __restrict__ ctr, BfsState::Published* pub, unsigned long long seq) {
+  bu_wide_body<kWords, kFirst, kSparse, kSpec>(cur, nxt, W, row_ptr, col, fpair, inv, pidx, pred,
+                                               level, ctr);
   publish_if_last(ctr, pub, seq);
 }
 
+template <int kClaim = 0>
 __global__ void __launch_bounds__(256) td_vec_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
     const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_vec_body(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
+  td_vec_body<kClaim>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
@@ -1333,16 +1349,14 @@ __global__ void __launch_bounds__(256) sg_td_kernel(
 template <bool kFirst>
 __global__ void __launch_bounds__(256, 4) sg_bu_kernel(
     const SingleCtl* __restrict__ c, int64_t W, const int64_t* __restrict__ row_ptr,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ first,
-    const int32_t* __restrict__ finv, const int32_t* __restrict__ inv,
-    const int32_t* __restrict__ pidx, uint32_t* const* __restrict__ vis_pp,
-    int64_t* __restrict__ pred, Counters* __restrict__ ctr) {
+    const int32_t* __restrict__ col, const int2* __restrict__ fpair,
+    const int32_t* __restrict__ inv, const int32_t* __restrict__ pidx,
+    uint32_t* const* __restrict__ vis_pp, int64_t* __restrict__ pred,
+    Counters* __restrict__ ctr) {
   if (c->done || c->forward) return;
   const int cur = c->cur;
-  bu_wide_body<4, kFirst, false>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, first, finv, inv,
-                                 pidx,
-                          pred,
-                          c->level, ctr);
+  bu_wide_body<4, kFirst, false>(vis_pp[cur], vis_pp[cur ^ 1], W, row_ptr, col, fpair, inv, pidx,
+                                 pred, c->level, ctr);
 }
 
 // kAfterBu = false: after a top-down level; true: after a bottom-up level
@@ -1603,8 +1617,8 @@ void sg_launch_level(const Graph& g, BfsState& st, cudaStream_t s, int sms, int 
                                                                           st.queue, st.qdeg,
                                                              st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                                              st.d_vis, out);
-  (bu_first && c.first ? sg_bu_kernel<true> : sg_bu_kernel<false>)<<<sms * 4, B, 0, s>>>(
-      st.sctl, st.W, c.row_ptr, c.col, c.first, c.first_inv, c.inv, pidx, st.d_vis, out, st.ctr);
+  (bu_first && c.first_pair ? sg_bu_kernel<true> : sg_bu_kernel<false>)<<<sms * 4, B, 0, s>>>(
+      st.sctl, st.W, c.row_ptr, c.col, c.first_pair, c.inv, pidx, st.d_vis, out, st.ctr);
   sg_count_kernel<false><<<nblk, kFrontierThreads, 0, s>>>(st.sctl, st.d_vis, st.fr, st.W,
                                                          c.row_ptr, c.mdeg, st.blk_cnt,
                                                          st.blk_deg, st.ctr);
@@ -1628,7 +1642,7 @@ std::vector<const void*> sg_key(const Graph& g, const BfsState& st, int sms, int
           (const void*)(intptr_t)st.W, (const void*)(intptr_t)st.R,
           (const void*)(intptr_t)st.pred_size, (const void*)(intptr_t)c.nedges,
           (const void*)(intptr_t)sms, (const void*)(intptr_t)td_form,
-          (const void*)(intptr_t)force_direction, c.first, c.first_inv,
+          (const void*)(intptr_t)force_direction, c.first, c.first_pair,
           (const void*)(intptr_t)bu_first,
           (const void*)(intptr_t)assemble, st.rp, st.pmap};
 }
@@ -1866,8 +1880,20 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
         kernel<<<grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                   st.vis[cur], out, level);
       };
-      if (td_form == 6)
-        launch_td(td_vec_kernel, 0);
+      if (td_form == 6 && opt.td_claim == 1)
+        launch_td(td_vec_kernel<1>, 0);
+      else if (td_form == 6 && opt.td_claim == 2)
+        launch_td(td_vec_kernel<2>, 0);
+      else if (td_form == 6 && opt.td_claim == 3)
+        launch_td(td_vec_kernel<3>, 0);
+      else if (td_form == 6)
+        launch_td(td_vec_kernel<0>, 0);
+      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 1)
+        launch_td(td_expand_kernel<true, 1, 1>, 0);
+      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 2)
+        launch_td(td_expand_kernel<true, 1, 2>, 0);
+      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 3)
+        launch_td(td_expand_kernel<true, 1, 3>, 0);
       else if (td_form == 5 && opt.td_unroll == 4)
         launch_td(td_expand_kernel<true, 4>, 0);
       else if (td_form == 5 && opt.td_unroll == 2)
@@ -1889,10 +1915,10 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
     } else {
       ++rs.num_bu_levels;
       if (level < 64) rs.bu_level_mask |= 1ull << level;
-      const bool first = opt.bu_first && c.first;
+      const bool first = opt.bu_first && c.first_pair;
       auto launch_wide = [&](auto kernel, int grid) {
-        kernel<<<grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col, c.first,
-                                  c.first_inv, c.inv, pidx, out, level, st.ctr, st.dpub,
+        kernel<<<grid, B, 0, s>>>(st.vis[cur], st.vis[cur ^ 1], st.W, c.row_ptr, c.col,
+                                  c.first_pair, c.inv, pidx, out, level, st.ctr, st.dpub,
                                   st.pub_seq + 1);
       };
       auto launch_bu = [&](auto kernel) {
@@ -1902,20 +1928,29 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
       // the last levels, with few unvisited rows left, skip full bitmap words
       // 32 at a time (fewer than one unvisited row per four words)
       const bool sparse = opt.bu_sparse && 4 * (st.R - visited) < st.W;
+      // the levels where most rows are still unvisited load every row's
+      // first-neighbour entry beside its bitmap word
+      const bool spec = first && opt.bu_spec && 2 * (st.R - visited) > st.R;
       if (opt.bu_kernel == 2 && sparse)
         launch_wide(first ? bu_wide_kernel<2, 8, true, true> : bu_wide_kernel<2, 8, false, true>,
                     bu_wide_grid);
+      else if (opt.bu_kernel == 2 && spec)
+        launch_wide(bu_wide_kernel<2, 8, true, false, true>, bu_wide_grid);
       else if (opt.bu_kernel == 2)
         launch_wide(first ? bu_wide_kernel<2, 8, true> : bu_wide_kernel<2, 8, false>,
                     bu_wide_grid);
       else if (opt.bu_kernel == 3 && sparse)
         launch_wide(first ? bu_wide_kernel<2, 6, true, true> : bu_wide_kernel<2, 6, false, true>,
                     sms * 6);
+      else if (opt.bu_kernel == 3 && spec)
+        launch_wide(bu_wide_kernel<2, 6, true, false, true>, sms * 6);
       else if (opt.bu_kernel == 3)
         launch_wide(first ? bu_wide_kernel<2, 6, true> : bu_wide_kernel<2, 6, false>, sms * 6);
       else if (opt.bu_kernel == 4 && sparse)
         launch_wide(first ? bu_wide_kernel<4, 4, true, true> : bu_wide_kernel<4, 4, false, true>,
                     sms * 4);
+      else if (opt.bu_kernel == 4 && spec)
+        launch_wide(bu_wide_kernel<4, 4, true, false, true>, sms * 4);
       else if (opt.bu_kernel == 4)
         launch_wide(first ? bu_wide_kernel<4, 4, true> : bu_wide_kernel<4, 4, false>, sms * 4);
       else if (opt.bu_probe <= 4)

@@ -179,12 +179,12 @@ __global__ void compact_rows_kernel(const int32_t* __restrict__ raw,
 
 __global__ void first_kernel(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
                              const int32_t* __restrict__ inv, int64_t R,
-                             int32_t* __restrict__ first, int32_t* __restrict__ first_inv) {
+                             int32_t* __restrict__ first, int2* __restrict__ first_pair) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < R;
        r += (int64_t)gridDim.x * blockDim.x) {
     const int32_t f = row_ptr[r + 1] > row_ptr[r] ? col[row_ptr[r]] : -1;
     first[r] = f;
-    if (first_inv) first_inv[r] = f >= 0 ? inv[f] : -1;
+    if (first_pair) first_pair[r] = make_int2(f, f >= 0 ? inv[f] : -1);
   }
 }
 
@@ -419,12 +419,12 @@ void build_csr(DeviceArena& arena, cudaStream_t s, const uint2* edges, int64_t m
 
 void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms, bool parent_ids) {
   arena.free(c.first);
-  arena.free(c.first_inv);
-  c.first_inv = nullptr;
+  arena.free(c.first_pair);
+  c.first_pair = nullptr;
   c.first = arena_alloc<int32_t>(arena, c.nrows, "first neighbours");
-  if (parent_ids) c.first_inv = arena_alloc<int32_t>(arena, c.nrows, "first neighbour ids");
+  if (parent_ids) c.first_pair = arena_alloc<int2>(arena, c.nrows, "first neighbour pairs");
   first_kernel<<<grid_for(c.nrows, 256, sms, 16), 256, 0, s>>>(c.row_ptr, c.col, c.inv, c.nrows,
-                                                               c.first, c.first_inv);
+                                                               c.first, c.first_pair);
   check_cuda(cudaGetLastError(), "first neighbours");
 }
 

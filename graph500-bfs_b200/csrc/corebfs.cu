@@ -382,7 +382,7 @@ void build_core(DeviceArena& arena, cudaStream_t s, Graph& g, int sms) {
   arena.free(c.rank);
   arena.free(c.mdeg);
   arena.free(c.first);
-  arena.free(c.first_inv);
+  arena.free(c.first_pair);
   c = k2;
   build_first(arena, s, c, sms);
   k.enabled = true;

@@ -91,10 +91,11 @@ struct Csr {
   // reference keeps each row's first edge apart too: isolated_edges_,
   // graph_constructor.hpp:1224-1348)
   int32_t* first = nullptr;
-  // [R] original id of the first neighbour (inv[first[r]]), read beside
-  // first[] so that a bottom-up parent found by the first probe needs no
-  // random gather into inv[] for the pred entry (null in the batch view)
-  int32_t* first_inv = nullptr;
+  // [R] (first[r], inv[first[r]]): the first neighbour and its original
+  // id in one 8-byte entry, so that the single-root bottom-up search gets
+  // both with one load and a parent found by the first probe needs neither
+  // a second load nor a random gather into inv[] (null in the batch view)
+  int2* first_pair = nullptr;
   int64_t max_degree = 0;
 };
 
@@ -129,7 +130,7 @@ struct Graph {
   int64_t device_bytes = 0;
 };
 
-// Fills c.first from c.row_ptr and c.col, and c.first_inv when parent_ids.
+// Fills c.first from c.row_ptr and c.col, and c.first_pair when parent_ids.
 void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms, bool parent_ids = true);
 
 // Builds g.csr from nedges device edges (each a (v0, v1) pair of uint32 ids).

@@ -38,7 +38,7 @@ struct Engine {
     arena.free(g.csr.rank);
     arena.free(g.csr.mdeg);
     arena.free(g.csr.first);
-    arena.free(g.csr.first_inv);
+    arena.free(g.csr.first_pair);
     arena.free(g.input_edges);
     g = Graph();
   }

@@ -285,7 +285,13 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * 1), "bu_first" (1: bottom-up forms 2-4 probe the first neighbour from a
  * dense per-row array first, the default), "bu_sparse" (1: on levels with
  * few unvisited rows bottom-up forms 2-4 skip full bitmap words 32 at a time,
- * the default; 0: every word steps through the row search), "td_unroll" (1, 2 or 4: 32-entry
+ * the default; 0: every word steps through the row search), "bu_spec" (1: on
+ * levels where more than half of the rows are unvisited bottom-up forms 2-4
+ * load every row's first-neighbour entry beside its bitmap word, the
+ * default; 0: only the unvisited rows' entries, after the word), "td_claim"
+ * (0..3, top-down forms 5 and 6: bit 0 reads the visited words from L2
+ * only, bit 1 claims with an atomic OR that returns the old word so that
+ * only the setter writes pred), "td_unroll" (1, 2 or 4: 32-entry
  * steps a lane of top-down form 5 handles together), "pred_assemble" (1:
  * the levels write a row-order buffer and one pass over the original ids
  * writes pred, the default; after a search of this kind the pass leaves out

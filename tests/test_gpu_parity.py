@@ -470,16 +470,20 @@ def test_find_roots_matches_oracle(engine, oracle_graphs, scale, flags):
         assert np.array_equal(dev, ref), (r1, r2)
 
 
-@pytest.mark.parametrize("bu,sparse", [(2, 0), (2, 1), (3, 1), (4, 1), (4, 0)])
-def test_bottom_up_sparse_levels_agree(engine, oracle_graphs, bu, sparse):
+@pytest.mark.parametrize("bu,sparse,spec", [(2, 0, 0), (2, 1, 0), (2, 1, 1), (2, 0, 1), (3, 1, 0),
+                                             (3, 1, 1), (4, 1, 0), (4, 1, 1), (4, 0, 0)])
+def test_bottom_up_sparse_levels_agree(engine, oracle_graphs, bu, sparse, spec):
     """Bottom-up forms with (bu_sparse 1) and without the skip of full
-    bitmap words on levels with few unvisited rows; every level after the
-    first runs bottom-up (force_direction 2), so the last levels take the
-    sparse path."""
+    bitmap words on levels with few unvisited rows, and form 2 with and
+    without the early first-neighbour loads on levels where most rows are
+    unvisited (bu_spec); every level after the first runs bottom-up
+    (force_direction 2), so the second level takes the early-load path and
+    the last levels the sparse path."""
     edges, g = oracle_graphs(18)
     engine.generate_graph(18, 16)
     engine.set_option("bu_kernel", bu)
     engine.set_option("bu_sparse", sparse)
+    engine.set_option("bu_spec", spec)
     engine.set_option("force_direction", 2)
     engine.prepare(16)
     try:
@@ -491,5 +495,6 @@ def test_bottom_up_sparse_levels_agree(engine, oracle_graphs, bu, sparse):
     finally:
         engine.set_option("bu_kernel", 2)
         engine.set_option("bu_sparse", 1)
+        engine.set_option("bu_spec", 1)
         engine.set_option("force_direction", 0)
         engine.end()
