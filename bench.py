@@ -247,6 +247,28 @@ def pick_roots(eng, args):
     return roots, np.array(nedge, dtype=np.float64), cold_ms
 
 
+def td_random_access(eng, info, stats, td_ms, stream):
+    """The top-down kernels against the random-access ceiling: probes per
+    second (b200bfs_random_access_rate, loads and ORs into a buffer of the
+    visited bitmap's size, rounded up to a power of two) and the probe-only
+    time the searches' top-down entries would take at that rate."""
+    import torch
+    import b200bfs
+    words = max(1, (info.num_rows + 31) // 32)
+    log2w = max(10, (words - 1).bit_length())
+    buf = torch.zeros(1 << log2w, dtype=torch.int32, device="cuda")
+    loads = b200bfs.random_access_rate(buf.data_ptr(), log2w, 0, stream.cuda_stream)
+    ors = b200bfs.random_access_rate(buf.data_ptr(), log2w, 1, stream.cuda_stream)
+    del buf
+    entries = sum(s.edges_scanned_td for s in stats)
+    ceiling_ms = 1e3 * entries / loads
+    return {"buffer_bytes": 4 << log2w, "loads_per_s": loads, "ors_per_s": ors,
+            "entries_per_search": entries / len(stats),
+            "entries_per_s": entries / (td_ms / 1e3) if td_ms > 0 else 0.0,
+            "probe_ceiling_ms_per_search": ceiling_ms / len(stats),
+            "frac": ceiling_ms / td_ms if td_ms > 0 else None}
+
+
 def harmonic_teps(nedge, times):
     return len(times) / float(np.sum(np.asarray(times) / np.asarray(nedge)))
 
@@ -720,6 +742,14 @@ def main():
                              "frac": gbs / peak,
                              "share_of_search_time": ms / (1e3 * sum(times)),
                              "traffic": ncu_traffic(name)}
+    # The top-down levels are random 4-byte probes of the visited bitmap (one
+    # per adjacency entry) and ORs (one per claim): the device's rate of such
+    # accesses into a buffer the size of that bitmap, measured here, bounds
+    # them where the HBM bandwidth does not.  ceiling_ms counts the probes
+    # only, so the fraction is a lower bound.
+    if "td_expand_kernel" in kernels:
+        kernels["td_expand_kernel"]["random_access"] = td_random_access(
+            eng, info, stats, td_ms, stream)
 
     line = {
         "metric": f"harmonic-mean GTEPS, SCALE {args.scale}; 64-root batched BFS/s + p99 vs 1-root",

@@ -45,6 +45,7 @@ SYMBOLS = [
     "b200bfs_server_submit", "b200bfs_server_poll", "b200bfs_server_wait",
     "b200bfs_server_get_levels", "b200bfs_server_release", "b200bfs_server_get_stats",
     "b200bfs_server_reset_stats", "b200bfs_server_last_error", "b200bfs_server_stop",
+    "b200bfs_random_access_rate",
 ]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(5)
 BATCH_MAX = 64  # B200BFS_BATCH_MAX
@@ -187,6 +188,7 @@ def load_library(path=LIB_PATH):
     L.b200bfs_validate_pred.argtypes = [H, i64, ctypes.c_void_p, ctypes.c_int,
                                         P(ctypes.c_int64), P(ctypes.c_int64)]
     L.b200bfs_bfs_noalloc.argtypes = [vp, vp, i64, i64, vp, vp, P(ctypes.c_int32)]
+    L.b200bfs_random_access_rate.argtypes = [vp, i32, i32, vp, P(dbl)]
     L.b200bfs_run_batch.argtypes = [H, vp, i32, i32, dbl, dbl, P(BatchStats)]
     L.b200bfs_tune_engine.argtypes = [H, vp, i32, i32, dbl, dbl, i32, P(TuneReport)]
     L.b200bfs_batch_select.argtypes = [H, i32]
@@ -408,6 +410,19 @@ class Engine:
 
 
 NOALLOC_MAX_ROWS = 1 << 24  # B200BFS_NOALLOC_MAX_ROWS
+
+
+def random_access_rate(words_dev, log2_words, kind, stream=0):
+    """b200bfs_random_access_rate on a device buffer (int pointer) of
+    2^log2_words uint32: random 4-byte loads (kind 0) or non-returning ORs
+    (kind 1) per second on the current device."""
+    L = load_library()
+    out = ctypes.c_double(0)
+    rc = L.b200bfs_random_access_rate(ctypes.c_void_p(words_dev), log2_words, kind,
+                                      ctypes.c_void_p(stream), ctypes.byref(out))
+    if rc:
+        raise B200BfsError(rc, "b200bfs_random_access_rate failed")
+    return out.value
 
 
 def bfs_noalloc(row_ptr_dev, col_dev, nrows, root, pred_dev, stream=0):

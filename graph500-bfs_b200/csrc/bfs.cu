@@ -132,12 +132,18 @@ __global__ void reset_unvisited_kernel(const uint32_t* __restrict__ vis, int64_t
 // contiguous, so the rp reads of the ids a wave of warps covers fall in a few
 // windows that stay in L2.  Scattering the entries by original id during the
 // levels instead costs a random 32-byte sector per entry.
+// A row's visited word and rp entry are loaded together (both only for
+// rows), so the entry costs one round trip after the map; nearly every row
+// is reached in a search of the giant component, so the rp reads of the
+// unreached rows are few.
 __device__ __forceinline__ int64_t assembled_entry(int32_t m, int64_t u,
                                                    const uint32_t* __restrict__ vis,
                                                    const int64_t* __restrict__ rp, int64_t root) {
   int64_t e = -1;
   if (m >= 0) {
-    if ((__ldg(vis + (m >> 5)) >> (m & 31)) & 1u) e = __ldg(rp + m);
+    const uint32_t vw = __ldg(vis + (m >> 5));
+    const int64_t r = __ldg(rp + m);
+    if ((vw >> (m & 31)) & 1u) e = r;
   } else if (m < -1) {
     e = pred_entry(-(int64_t)m - 2, 0xFFFF);
   }
@@ -219,33 +225,22 @@ __global__ void pred_map_kernel(const int32_t* __restrict__ rank, const int32_t*
 // kUnroll: 32-entry steps handled together by a lane (all neighbour ids of
 // the steps loaded, then all visited probes, then the claims), so more
 // independent loads are in flight.
-// How a top-down entry probes and claims its neighbour u (kClaim bits).
-// Bit 0: the visited word is read from L2 (ld.global.cg) instead of through
-// L1, whose lines do not see the ORs other warps make during the level.
-// Bit 1: an unvisited u is claimed with an atomic OR that returns the old
-// word, and only the warp lane that set the bit writes u's pred entry;
-// without it every entry that saw u unvisited writes (a redundant but valid
-// parent) and ORs without a return.
-template <int kClaim>
-__device__ __forceinline__ uint32_t td_probe(const uint32_t* vis, int32_t u) {
-  return (kClaim & 1) ? __ldcg(vis + (u >> 5)) : vis[u >> 5];
-}
-
-template <int kClaim>
-__device__ __forceinline__ void td_claim_as(int32_t u, uint32_t word, int64_t entry,
-                                            const int32_t* __restrict__ pidx, uint32_t* vis,
-                                            int64_t* __restrict__ pred) {
+// Claim of neighbour u by a top-down entry whose probe read the visited
+// word `word`: an unvisited u gets the entry's pred entry and its visited
+// bit.  Several entries may claim the same u in one level (a probe can read
+// a word before another warp's OR reaches it, or a stale L1 line); each
+// writes a valid parent of the same level, and the OR has no return.
+__device__ __forceinline__ void td_claim(int32_t u, uint32_t word, int64_t entry,
+                                         const int32_t* __restrict__ pidx, uint32_t* vis,
+                                         int64_t* __restrict__ pred) {
   const uint32_t bit = 1u << (u & 31);
-  if ((word & bit) != 0) return;
-  if (kClaim & 2) {
-    if ((atomicOr(vis + (u >> 5), bit) & bit) == 0) pred[pred_slot(pidx, u)] = entry;
-  } else {
+  if ((word & bit) == 0) {
     pred[pred_slot(pidx, u)] = entry;
     red_or(vis + (u >> 5), bit);
   }
 }
 
-template <bool kWarpSearch, int kUnroll, int kClaim = 0>
+template <bool kWarpSearch, int kUnroll>
 __device__ __forceinline__ void td_expand_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -304,14 +299,13 @@ __device__ __forceinline__ void td_expand_body(
       // causes a redundant (still valid) claim
       uint32_t words[kUnroll];
 #pragma unroll
-      for (int j = 0; j < kUnroll; ++j) words[j] = us[j] >= 0 ? td_probe<kClaim>(vis, us[j]) : kFull;
+      for (int j = 0; j < kUnroll; ++j) words[j] = us[j] >= 0 ? vis[us[j] >> 5] : kFull;
 #pragma unroll
       for (int j = 0; j < kUnroll; ++j) {
         if (us[j] < 0) continue;
         const uint32_t bit = 1u << (us[j] & 31);
         if ((words[j] & bit) == 0)
-          td_claim_as<kClaim>(us[j], words[j], pred_entry(__ldg(inv + srcs[j]), level), pidx, vis,
-                              pred);
+          td_claim(us[j], words[j], pred_entry(__ldg(inv + srcs[j]), level), pidx, vis, pred);
       }
     }
   }
@@ -851,7 +845,6 @@ __device__ __forceinline__ void td_chunk_body(
 // for the next step.
 constexpr int kVecTile = 1024;  // entries per warp tile: 8 steps of 128
 
-template <int kClaim = 0>
 __device__ __forceinline__ void td_vec_body(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
@@ -901,12 +894,12 @@ __device__ __forceinline__ void td_vec_body(
         }
         // plain loads: vis is being updated by this kernel; a stale word
         // only causes a redundant (still valid) claim
-        const uint32_t w0 = td_probe<kClaim>(vis, u0), w1 = td_probe<kClaim>(vis, u1),
-                       w2 = td_probe<kClaim>(vis, u2), w3 = td_probe<kClaim>(vis, u3);
-        td_claim_as<kClaim>(u0, w0, entry, pidx, vis, pred);
-        td_claim_as<kClaim>(u1, w1, entry, pidx, vis, pred);
-        td_claim_as<kClaim>(u2, w2, entry, pidx, vis, pred);
-        td_claim_as<kClaim>(u3, w3, entry, pidx, vis, pred);
+        const uint32_t w0 = vis[u0 >> 5], w1 = vis[u1 >> 5], w2 = vis[u2 >> 5],
+                       w3 = vis[u3 >> 5];
+        td_claim(u0, w0, entry, pidx, vis, pred);
+        td_claim(u1, w1, entry, pidx, vis, pred);
+        td_claim(u2, w2, entry, pidx, vis, pred);
+        td_claim(u3, w3, entry, pidx, vis, pred);
         continue;
       }
       // the step crosses a row boundary: per-lane walk over 32-entry sub-steps
@@ -925,8 +918,7 @@ __device__ __forceinline__ void td_vec_body(
             l_rb = row_ptr[l_src];
           }
           const int32_t u = __ldg(col + l_rb + (e - l_lo));
-          td_claim_as<kClaim>(u, td_probe<kClaim>(vis, u), pred_entry(__ldg(inv + l_src), level),
-                              pidx, vis, pred);
+          td_claim(u, vis[u >> 5], pred_entry(__ldg(inv + l_src), level), pidx, vis, pred);
         }
       }
       // lane 31 walked furthest (to the row of entry e0 + 127, when the tile
@@ -1159,15 +1151,14 @@ __device__ __forceinline__ void frontier_write_body(
 
 // Kernels of the host-driven level loop: thin wrappers around the bodies
 // above, which the device-driven loop (below) shares.
-template <bool kWarpSearch, int kUnroll, int kClaim = 0>
+template <bool kWarpSearch, int kUnroll>
 __global__ void __launch_bounds__(256) td_expand_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
     const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_expand_body<kWarpSearch, kUnroll, kClaim>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred,
-                                               level);
+  td_expand_body<kWarpSearch, kUnroll>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 template <int kWords, int kMinBlocks, bool kFirst, bool kSparse = false, bool kSpec = false>
@@ -1182,14 +1173,13 @@ __global__ void __launch_bounds__(256, kMinBlocks) bu_wide_kernel(
   publish_if_last(ctr, pub, seq);
 }
 
-template <int kClaim = 0>
 __global__ void __launch_bounds__(256) td_vec_kernel(
     const int32_t* __restrict__ queue, const int64_t* __restrict__ qdeg,
     const Counters* __restrict__ ctr, const int64_t* __restrict__ row_ptr,
     const int32_t* __restrict__ col, const int32_t* __restrict__ inv,
     const int32_t* __restrict__ pidx, uint32_t* vis,
     int64_t* __restrict__ pred, int64_t level) {
-  td_vec_body<kClaim>(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
+  td_vec_body(queue, qdeg, ctr, row_ptr, col, inv, pidx, vis, pred, level);
 }
 
 __global__ void __launch_bounds__(256) td_chunk_kernel(
@@ -1880,20 +1870,8 @@ void run_bfs_core(const Graph& g, BfsState& st, cudaStream_t s, int sms, int64_t
         kernel<<<grid, B, 0, s>>>(st.queue, st.qdeg, st.ctr, c.row_ptr, c.col, c.inv, pidx,
                                   st.vis[cur], out, level);
       };
-      if (td_form == 6 && opt.td_claim == 1)
-        launch_td(td_vec_kernel<1>, 0);
-      else if (td_form == 6 && opt.td_claim == 2)
-        launch_td(td_vec_kernel<2>, 0);
-      else if (td_form == 6 && opt.td_claim == 3)
-        launch_td(td_vec_kernel<3>, 0);
-      else if (td_form == 6)
-        launch_td(td_vec_kernel<0>, 0);
-      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 1)
-        launch_td(td_expand_kernel<true, 1, 1>, 0);
-      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 2)
-        launch_td(td_expand_kernel<true, 1, 2>, 0);
-      else if (td_form == 5 && opt.td_unroll == 1 && opt.td_claim == 3)
-        launch_td(td_expand_kernel<true, 1, 3>, 0);
+      if (td_form == 6)
+        launch_td(td_vec_kernel, 0);
       else if (td_form == 5 && opt.td_unroll == 4)
         launch_td(td_expand_kernel<true, 4>, 0);
       else if (td_form == 5 && opt.td_unroll == 2)

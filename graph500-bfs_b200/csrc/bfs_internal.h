@@ -127,10 +127,7 @@ struct RunOptions {
   // unvisited: load every row's first-neighbour entry beside its bitmap
   // word (1) or only the unvisited rows' entries once the word is in (0)
   int bu_spec = 1;
-  int td_unroll = 1;
-  // top-down forms 5 and 6: visited probes through L2 only (bit 0), claims
-  // by an atomic OR with return so that only the setter writes pred (bit 1)
-  int td_claim = 0;        // td form 5: 32-entry steps per lane handled together (1, 2, 4)
+  int td_unroll = 1;        // td form 5: 32-entry steps per lane handled together (1, 2, 4)
   int force_direction = 0;  // 0: alpha/beta rule, 1: top-down only, 2: bottom-up after level 1
   // pred output.  1: the level kernels write a row-order buffer and one
   // pass over the original ids assembles pred (sequential pred writes); 0:

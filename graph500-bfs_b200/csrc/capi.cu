@@ -554,9 +554,6 @@ int b200bfs_set_option(b200bfs_handle* h, const char* name, int64_t value) {
     } else if (n == "bu_sparse") {
       require(value == 0 || value == 1, B200BFS_ERR_INVALID, "bu_sparse must be 0 or 1");
       e.opt.bu_sparse = (int)value;
-    } else if (n == "td_claim") {
-      require(value >= 0 && value <= 3, B200BFS_ERR_INVALID, "td_claim must be 0..3");
-      e.opt.td_claim = (int)value;
     } else if (n == "bu_spec") {
       require(value == 0 || value == 1, B200BFS_ERR_INVALID, "bu_spec must be 0 or 1");
       e.opt.bu_spec = (int)value;

@@ -288,10 +288,7 @@ int b200bfs_tune_engine(b200bfs_handle* h, const int64_t* roots, int num_roots, 
  * the default; 0: every word steps through the row search), "bu_spec" (1: on
  * levels where more than half of the rows are unvisited bottom-up forms 2-4
  * load every row's first-neighbour entry beside its bitmap word, the
- * default; 0: only the unvisited rows' entries, after the word), "td_claim"
- * (0..3, top-down forms 5 and 6: bit 0 reads the visited words from L2
- * only, bit 1 claims with an atomic OR that returns the old word so that
- * only the setter writes pred), "td_unroll" (1, 2 or 4: 32-entry
+ * default; 0: only the unvisited rows' entries, after the word), "td_unroll" (1, 2 or 4: 32-entry
  * steps a lane of top-down form 5 handles together), "pred_assemble" (1:
  * the levels write a row-order buffer and one pass over the original ids
  * writes pred, the default; after a search of this kind the pass leaves out
@@ -494,6 +491,22 @@ int b200bfs_server_stop(b200bfs_server* srv);
  * caller. */
 int b200bfs_bfs_noalloc(const int64_t* row_ptr, const int32_t* col, int64_t nrows,
                         int64_t root, int64_t* pred, void* stream, int32_t* num_levels);
+
+/* ------------------------------ measurement ------------------------------ */
+
+/* No counterpart in the reference (a measurement aid): the rate at which
+ * this GPU's SMs issue independent random 4-byte accesses into `words`, a
+ * caller-owned device buffer of 2^log2_words uint32 (10 <= log2_words <= 30;
+ * its contents are overwritten when kind is 1): kind 0 loads, kind 1
+ * non-returning ORs.  These are the accesses a top-down level is made of (a
+ * visited-bitmap probe per adjacency entry, an OR per claim), so with a
+ * buffer the size of the visited bitmap the result is the ceiling the
+ * top-down kernels are measured against.  Enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) and synchronised; *per_s
+ * receives accesses per second (the best of three launches after one
+ * warm-up).  Allocates nothing. */
+int b200bfs_random_access_rate(void* words, int log2_words, int kind, void* stream,
+                               double* per_s);
 
 #ifdef __cplusplus
 }
