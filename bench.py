@@ -723,6 +723,7 @@ def main():
     achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                "frac_of_nominal_8000_gbs": achieved / 8000.0,
                 "traffic": ncu_traffic(kname),
                 "algorithmic_bytes_per_launch": kbytes / max(launches, 1),
                 "launches": launches, "share_of_search_time":
@@ -739,7 +740,7 @@ def main():
         if ms > 0:
             gbs = nbytes / (ms / 1e3) / 1e9
             kernels[name] = {"ms_per_search": ms / len(stats), "achieved_gbs": gbs,
-                             "frac": gbs / peak,
+                             "frac": gbs / peak, "frac_of_nominal_8000_gbs": gbs / 8000.0,
                              "share_of_search_time": ms / (1e3 * sum(times)),
                              "traffic": ncu_traffic(name)}
     # The top-down levels are random 4-byte probes of the visited bitmap (one
