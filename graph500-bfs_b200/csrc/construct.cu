@@ -422,7 +422,15 @@ void build_first(DeviceArena& arena, cudaStream_t s, Csr& c, int sms, bool paren
   arena.free(c.first_pair);
   c.first_pair = nullptr;
   c.first = arena_alloc<int32_t>(arena, c.nrows, "first neighbours");
-  if (parent_ids) c.first_pair = arena_alloc<int2>(arena, c.nrows, "first neighbour pairs");
+  if (parent_ids) {
+    // rounded up to whole 32-row bitmap words: the bottom-up sweep's early
+    // loads read the entries of all 32 rows of a word, the last word's
+    // padding rows included (their entries are discarded); the padding
+    // holds (-1, -1)
+    const int64_t padded = (c.nrows + 31) / 32 * 32;
+    c.first_pair = arena_alloc<int2>(arena, padded, "first neighbour pairs");
+    check_cuda(cudaMemsetAsync(c.first_pair, 0xFF, padded * sizeof(int2), s), "memset");
+  }
   first_kernel<<<grid_for(c.nrows, 256, sms, 16), 256, 0, s>>>(c.row_ptr, c.col, c.inv, c.nrows,
                                                                c.first, c.first_pair);
   check_cuda(cudaGetLastError(), "first neighbours");
